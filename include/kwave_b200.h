@@ -1,0 +1,212 @@
+/*
+ * kwave_b200.h -- C ABI of the B200 k-space pseudospectral acoustic solver.
+ *
+ * This library is a drop-in for the external solver binaries that k-Wave's
+ * C/G-suffixed MATLAB functions call (kspaceFirstOrder-OMP / -CUDA).  The
+ * reference defines that boundary by three things, and each entry point
+ * below replaces one of them:
+ *
+ *   1. the HDF5 input file that MATLAB writes
+ *      (k-Wave/private/kspaceFirstOrder_saveToDisk.m:44-378, writeMatrix.m);
+ *      -> struct kw_input holds exactly those datasets, in memory;
+ *   2. the command line that MATLAB passes to the binary
+ *      (k-Wave/kspaceFirstOrder3DC.m:462-545: -i, -o, --p_raw, --p_max, ...,
+ *      -s, -g, --verbose);
+ *      -> struct kw_options and kw_cli_main();
+ *   3. the output datasets MATLAB reads back
+ *      (k-Wave/kspaceFirstOrder3DC.m:569-776: /p, /p_max, /p_rms, /ux, ...);
+ *      -> struct kw_output.
+ *
+ * Arrays use the reference's MATLAB layout: a grid array is Nx*Ny*Nz values
+ * with x fastest (the HDF5 dataset (Nz, Ny, Nx) read in C order); linear
+ * indices are 1-based column-major, as MATLAB's find() returns them.  Time
+ * series are [time][point] (point fastest), i.e. MATLAB [Ns, Nt].
+ *
+ * Errors: every entry point returns a kw_status_code and, when `status` is
+ * non-NULL, a NUL-terminated message.  Inputs are validated on the host
+ * before any device work.  The library owns device memory; the caller owns
+ * every host buffer.
+ */
+#ifndef KWAVE_B200_H
+#define KWAVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KW_ABI_VERSION 1
+
+typedef enum {
+  KW_OK = 0,
+  KW_ERR_INVALID_ARGUMENT = 1,
+  KW_ERR_CUDA = 2,
+  KW_ERR_OUT_OF_MEMORY = 3,
+  KW_ERR_IO = 4,
+  KW_ERR_UNSUPPORTED = 5,
+  KW_ERR_INTERNAL = 6
+} kw_status_code;
+
+typedef struct {
+  int code;
+  char message[512];
+} kw_status;
+
+/* A float dataset that is either a scalar ([1,1,1]) or a full grid map.
+ * numel is 1 or Nx*Ny*Nz. */
+typedef struct {
+  const float* data;
+  uint64_t numel;
+} kw_field;
+
+/*
+ * In-memory copy of the HDF5 input file (file format 1.2), dataset by
+ * dataset (k-Wave/private/kspaceFirstOrder_saveToDisk.m:44-106, 177-378).
+ * Source signals are already scaled and p0 already smoothed, as MATLAB does
+ * before writing the file (kspaceFirstOrder_scaleSourceTerms.m,
+ * kspaceFirstOrder_inputChecking.m:1499-1553).
+ */
+typedef struct {
+  /* grid: Nz = 1 for a 2D simulation (saveToDisk.m:147-150) */
+  uint64_t Nx, Ny, Nz, Nt;
+  float dx, dy, dz, dt;
+  float c_ref;
+  uint64_t pml_x_size, pml_y_size, pml_z_size;
+  float pml_x_alpha, pml_y_alpha, pml_z_alpha;
+
+  /* medium */
+  kw_field c0;
+  kw_field rho0;
+  kw_field rho0_sgx, rho0_sgy, rho0_sgz; /* density on the staggered grids */
+  uint64_t nonlinear_flag;
+  kw_field BonA;
+  uint64_t absorbing_flag; /* 0 lossless, 1 power law, 2 stokes */
+  kw_field alpha_coeff;    /* dB / (MHz^y cm), as written by MATLAB */
+  float alpha_power;
+
+  /* initial pressure */
+  uint64_t p0_source_flag;
+  const float* p0_source_input; /* Nx*Ny*Nz */
+
+  /* pressure source: flag = number of signal samples */
+  uint64_t p_source_flag;
+  uint64_t p_source_mode; /* 0 dirichlet, 1 additive-no-correction, 2 additive */
+  uint64_t p_source_many; /* 0: one signal for all points, 1: one per point */
+  const uint64_t* p_source_index; /* 1-based linear indices */
+  uint64_t p_source_index_numel;
+  const float* p_source_input; /* [p_source_flag][1 or index_numel] */
+
+  /* velocity sources (share u_source_index) */
+  uint64_t ux_source_flag, uy_source_flag, uz_source_flag;
+  uint64_t u_source_mode;
+  uint64_t u_source_many;
+  const uint64_t* u_source_index;
+  uint64_t u_source_index_numel;
+  const float* ux_source_input;
+  const float* uy_source_input;
+  const float* uz_source_input;
+
+  /* sensor: type 0 = linear indices, 1 = cuboid corners */
+  uint64_t sensor_mask_type;
+  const uint64_t* sensor_mask_index; /* 1-based */
+  uint64_t sensor_mask_index_numel;
+  const uint64_t* sensor_mask_corners; /* 6 x K, 1-based [x1 y1 z1 x2 y2 z2] per cuboid */
+  uint64_t sensor_mask_corners_numel;  /* 6 * K */
+} kw_input;
+
+/* What to record, and run settings: the binary's command-line flags. */
+typedef struct {
+  int p_raw, p_max, p_min, p_rms, p_max_all, p_min_all, p_final;
+  int u_raw, u_max, u_min, u_rms, u_max_all, u_min_all, u_final;
+  int u_non_staggered_raw;
+  uint64_t start_index; /* -s, 1-based; 0 is read as 1 */
+  int device;           /* -g, CUDA device ordinal; -1: current device */
+  int verbose;          /* --verbose 0..2 */
+} kw_options;
+
+/*
+ * Caller-owned host buffers for the outputs, sized as kw_output_sizes()
+ * reports.  Pointers for outputs that were not requested may be NULL.
+ * Sensor outputs are in sensor order: the order of sensor_mask_index, or,
+ * for cuboids, the concatenation of each cuboid's points (x fastest).
+ */
+typedef struct {
+  float* p;                       /* [Nt_rec][Ns] */
+  float *p_max, *p_min, *p_rms;   /* [Ns] */
+  float *p_max_all, *p_min_all;   /* [Nx*Ny*Nz] */
+  float* p_final;                 /* [Nx*Ny*Nz] */
+  float *ux, *uy, *uz;            /* [Nt_rec][Ns] */
+  float *ux_max, *uy_max, *uz_max;
+  float *ux_min, *uy_min, *uz_min;
+  float *ux_rms, *uy_rms, *uz_rms;
+  float *ux_max_all, *uy_max_all, *uz_max_all;
+  float *ux_min_all, *uy_min_all, *uz_min_all;
+  float *ux_final, *uy_final, *uz_final;
+  float *ux_non_staggered, *uy_non_staggered, *uz_non_staggered; /* [Nt_rec][Ns] */
+} kw_output;
+
+typedef struct {
+  uint64_t num_sensor_points;    /* Ns */
+  uint64_t num_recorded_steps;   /* Nt_rec = Nt - start_index + 1 */
+  uint64_t grid_points;          /* Nx*Ny*Nz */
+  uint64_t device_bytes;         /* device memory the solve will allocate */
+} kw_output_sizes;
+
+/* Library version string. */
+const char* kw_version(void);
+
+/* Output sizes for an input / option pair (validates the input). */
+int kw_output_sizes_query(const kw_input* in, const kw_options* opt, kw_output_sizes* sizes,
+                          kw_status* status);
+
+/*
+ * Run one simulation from host buffers to host buffers: the whole job of
+ * `kspaceFirstOrder-CUDA -i in.h5 -o out.h5 <flags>` without the files
+ * (k-Wave/kspaceFirstOrder3DC.m:535-563 runs the binary; :569-776 reads
+ * its outputs).
+ */
+int kw_solve(const kw_input* in, const kw_options* opt, kw_output* out, kw_status* status);
+
+/*
+ * The file-based drop-in: read a k-Wave HDF5 input file, run, and write the
+ * output file that kspaceFirstOrder{2D,3D}{C,G} read back
+ * (k-Wave/kspaceFirstOrder3DC.m:544 builds this call).
+ */
+int kw_run_file(const char* input_h5, const char* output_h5, const kw_options* opt, kw_status* status);
+
+/* Command-line entry: the binary's argv, e.g.
+ * {"kspaceFirstOrder-B200", "-i", "in.h5", "-o", "out.h5", "--p_raw", "-s", "10"}.
+ * Returns the process exit code. */
+int kw_cli_main(int argc, char** argv);
+
+/*
+ * Resident simulations, for callers that keep inputs on the device and
+ * advance a simulation in steps (batching, serving, benchmarking).  Not a
+ * reference interface: the reference runs one whole solve per process.
+ */
+typedef struct kw_session kw_session;
+
+int kw_session_create(const kw_input* in, const kw_options* opt, kw_session** session, kw_status* status);
+/* Enqueue `nsteps` time steps (asynchronous on the session's stream). */
+int kw_session_advance(kw_session* s, uint64_t nsteps, kw_status* status);
+/* Device time of the last kw_session_advance() in ms (synchronises). */
+int kw_session_elapsed_ms(kw_session* s, float* ms, kw_status* status);
+/* Block until all queued work finished. */
+int kw_session_sync(kw_session* s, kw_status* status);
+/* Steps completed so far. */
+uint64_t kw_session_steps_done(const kw_session* s);
+/* Copy the outputs recorded so far into host buffers. */
+int kw_session_read(kw_session* s, kw_output* out, kw_status* status);
+/* The session's CUDA stream (a cudaStream_t), for event timing by callers. */
+void* kw_session_stream(kw_session* s);
+/* Number of kernel launches one time step issues (the hot-path kernels). */
+uint64_t kw_session_launches_per_step(const kw_session* s);
+void kw_session_destroy(kw_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KWAVE_B200_H */

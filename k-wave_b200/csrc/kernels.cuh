@@ -1,0 +1,169 @@
+// Device-side data structures shared by the solver kernels and the host
+// orchestrator.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fft_engine.cuh"
+
+namespace kwb {
+
+constexpr int kThreads = 256;
+
+// Grid geometry.  Real fields are stored x-fastest ([z][y][x], the column-
+// major order of the reference's MATLAB arrays); the half spectrum of a real
+// field is stored [z][y][kx] with kx in [0, nx/2] and a row pitch of nxp.
+struct Dims {
+  int nx, ny, nz;   // nz == 1 in 2D
+  int dim;          // 2 or 3
+  int nxh;          // nx / 2 + 1
+  int nxp;          // spectral row pitch (complex elements)
+  long long nrows;  // ny * nz
+  long long npts;   // nx * ny * nz
+};
+
+enum SpecOpKind {
+  OP_GRAD_POS = 0,   // i k_a exp(+i k_a d_a / 2) * kappa
+  OP_GRAD_NEG = 1,   // i k_a exp(-i k_a d_a / 2) * kappa
+  OP_NABLA1 = 2,     // |k|^(y-2)
+  OP_NABLA2 = 3,     // |k|^(y-1)
+  OP_SRC_KAPPA = 4,  // cos(c_ref |k| dt / 2)
+  OP_IDENTITY = 5,
+};
+
+struct SpecOp {
+  int kind;
+  int axis;
+};
+
+// 1D operator tables (built in FP64 on the host, stored FP32) and scalars
+// from which the non-separable k-space operators are generated per point.
+struct SpecTables {
+  const float* k2[3];        // squared wavenumber per axis, FFT order (x: nxh entries)
+  const float2* ddk_pos[3];  // i k exp(+i k d / 2), FFT order (x: nxh entries)
+  const float2* ddk_neg[3];  // i k exp(-i k d / 2)
+  float cdt2;                // c_ref * dt / 2
+  float ym2, ym1;            // alpha_power - 2, alpha_power - 1
+  float scale;               // 1 / (nx ny nz): the inverse-FFT normalisation
+};
+
+// A medium property that is either a full map or a scalar.
+struct Map {
+  const float* p;
+  float s;
+  __device__ __forceinline__ float at(long long i) const { return p ? __ldg(p + i) : s; }
+};
+
+// Time-step clock: `t` points at the device-resident 1-based time index of
+// the step being computed, so a captured step graph can be replayed.
+struct Clock {
+  const int* t;
+  int start;  // record start index (1-based)
+};
+
+// Sparse sources applied inside the X-row kernels.  Indices are sorted
+// 0-based linear indices; `slot` gives the signal row of each entry.
+struct SparseSource {
+  int n;             // number of source points (0: no sparse source)
+  const int* idx;    // sorted linear indices
+  const int* slot;   // signal row for each sorted entry
+  const float* sig;  // signal matrix [t][row] (row fastest)
+  int nrows_sig;     // rows in the signal matrix (1 or n)
+  int len;           // number of signal samples (active while t <= len)
+  int mode;          // 0 dirichlet (set), 1 additive without correction (add)
+};
+
+// Dense additive source field, added inside the update epilogue while
+// t <= len: field * sig[t-1] (sig == nullptr: field * 1).
+struct DenseSource {
+  const float* field;
+  const float* sig;
+  int len;
+};
+
+// Sensor recording.  `mode` 0: off; 1: every grid point is a sensor point
+// and the output slot is the linear index; 2: sorted sparse list with slots.
+struct Sensor {
+  int mode;
+  int ns;
+  const int* idx;
+  const int* slot;
+  float* raw;      // [nrec][ns] time series (nullptr: off)
+  float* vmax;     // per-point reductions (nullptr: off)
+  float* vmin;
+  float2* rms;     // Kahan sum of squares {sum, compensation}
+  float* max_all;  // full-grid reductions (nullptr: off)
+  float* min_all;
+};
+
+// ---------------------------------------------------------------------------
+// kernel argument blocks
+// ---------------------------------------------------------------------------
+struct ColArgs {
+  float2* buf[4];     // fields transformed in place (blockIdx.z)
+  int ncols;          // valid columns (kx values)
+  long long lstride;  // element stride along the transformed axis
+  long long ostride;  // stride of the outer index (blockIdx.y)
+  int tl;             // columns per tile
+};
+
+struct FusedArgs {
+  const float2* in[3];  // inputs (blockIdx.z)
+  float2* out[9];       // outputs [input * fanout + o]
+  SpecOp op[9];
+  int fanout;
+  int ncols;
+  long long lstride, ostride;
+  int tl;
+};
+
+struct UArgs {
+  const float2* S[3];  // gradient spectra, already inverse-transformed along y / z
+  float2* Sout[3];     // receives the x-transform of the new velocity
+  float* u[3];
+  Map rinv[3];         // 1 / rho0 on the staggered grids
+  const float* pml_sg[3];
+  float dt;
+  int init;            // 1: u = dt * rinv * grad / 2 (initial-pressure start)
+  int do_r2c;
+  SparseSource src;    // velocity sources share one index list ...
+  const float* src_sig[3];  // ... with one signal matrix per component
+  int src_len[3];
+  DenseSource dsrc[3];
+  Sensor sens[3];
+  Clock clk;
+};
+
+struct RhoArgs {
+  const float2* S[3];  // divergence spectra, inverse-transformed along y / z
+  float* rho[3];
+  Map rho0;
+  const float* pml[3];
+  float dt;
+  int nonlinear;
+  Map bona;
+  Map c0sq;
+  int eos;             // 0 lossless, 1 absorbing, 2 stokes
+  Map tau;             // stokes coefficient
+  SparseSource src;
+  DenseSource dsrc;
+  float* p_loc;        // absorbing: c0^2 (sum rho + B/A term)
+  float2* S_q;         // absorbing: x-transform of rho0 * sum(du)
+  float2* S_r;         // absorbing: x-transform of sum(rho)
+  float* p_out;        // lossless / stokes: p (nullptr: not stored)
+  float2* S_p;         // lossless / stokes: x-transform of p
+  Sensor sens;
+  Clock clk;
+};
+
+struct EosArgs {
+  const float2* S_a;   // F^-1{nabla1 F{rho0 sum du}} (x still transformed)
+  const float2* S_b;   // F^-1{nabla2 F{sum rho}}
+  const float* p_loc;
+  Map c2tau, c2eta;    // c0^2 tau, c0^2 eta
+  float* p_out;
+  float2* S_p;
+  Sensor sens;
+  Clock clk;
+};
+
+}  // namespace kwb

@@ -1,0 +1,982 @@
+// Host orchestrator and C ABI of the B200 k-space solver.
+//
+// A session owns one simulation resident in HBM: medium maps, the split
+// density and velocity fields, four half-spectrum work buffers, operator
+// tables and sensor accumulators.  kw_session_advance() enqueues time steps
+// on the session's stream; kw_solve() is create + advance(Nt) + read.
+//
+// The operators that the v1.2 input file omits are rebuilt here from the
+// scalars it carries (dx, dt, c_ref, pml_*), in FP64, then stored as FP32
+// 1D tables (k-Wave/kspaceFirstOrder3D.m:617-659, private/getPML.m:49-85,
+// kWaveGrid.m:779-797, kspaceFirstOrder_createAbsorptionVariables.m:27-99).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "kwave_b200.h"
+#include "solver_internal.h"
+
+namespace kwb {
+
+// launch helpers (kernels.cu)
+cudaError_t launch_col_fft(bool inv, const ColArgs& a, int nfields, long long nouter, const FFTPlan& plan,
+                           const float2* tw, cudaStream_t st);
+cudaError_t launch_fused_last(const FusedArgs& a, int ninputs, long long nouter, const FFTPlan& plan,
+                              const float2* tw, const SpecTables& T, int dim, cudaStream_t st);
+cudaError_t launch_x_u(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                       cudaStream_t st);
+cudaError_t launch_x_rho(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                         cudaStream_t st);
+cudaError_t launch_x_eos(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                         cudaStream_t st);
+cudaError_t launch_x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw,
+                         int L, cudaStream_t st);
+cudaError_t launch_x_c2r(const float2* S, float* out, int accumulate, const Dims& d, const FFTPlan& plan,
+                         const float2* tw, int L, cudaStream_t st);
+cudaError_t launch_scatter(float* f, const int* idx, const int* slot, int n, const float* sig,
+                           int nrows_sig, int t, cudaStream_t st);
+cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim,
+                            long long n, cudaStream_t st);
+cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& clk, long long n,
+                                cudaStream_t st);
+cudaError_t launch_advance(int* t, cudaStream_t st);
+cudaError_t launch_rms_final(const float2* acc, float* out, long long n, float inv_n, cudaStream_t st);
+
+static void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) throw KwError(KW_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    throw KwError(KW_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// device buffer
+// ---------------------------------------------------------------------------
+DevBuf::~DevBuf() {
+  if (p) cudaFree(p);
+}
+void DevBuf::alloc(size_t nbytes) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = nbytes;
+  if (nbytes == 0) return;
+  ck(cudaMalloc(&p, nbytes), "cudaMalloc");
+}
+
+// ---------------------------------------------------------------------------
+// FP64 operator construction
+// ---------------------------------------------------------------------------
+// centred wavenumbers (kWaveGrid.m:779-797) reordered with ifftshift
+static std::vector<double> kvec_fft_order(int n, double d) {
+  std::vector<double> c(n);
+  const int h = n / 2;
+  for (int j = 0; j < n; ++j) {
+    double nx = (n % 2 == 0) ? (double)(j - h) / n : (double)(j - (n - 1) / 2) / n;
+    c[j] = nx;
+  }
+  c[h] = 0.0;
+  std::vector<double> k(n);
+  for (int b = 0; b < n; ++b) k[b] = (2.0 * M_PI / d) * c[(b + h) % n];
+  return k;
+}
+
+// getPML.m:49-85 (non-axisymmetric)
+static std::vector<double> pml_profile(int n, double d, double dt, double c, int size, double alpha, bool stag) {
+  std::vector<double> pml(n, 1.0);
+  for (int i = 1; i <= size && size > 0; ++i) {
+    double x = i;
+    double left, right;
+    if (stag) {
+      left = alpha * (c / d) * std::pow(((x + 0.5) - size - 1) / (0.0 - size), 4);
+      right = alpha * (c / d) * std::pow((x + 0.5) / size, 4);
+    } else {
+      left = alpha * (c / d) * std::pow((x - size - 1) / (0.0 - size), 4);
+      right = alpha * (c / d) * std::pow(x / size, 4);
+    }
+    pml[i - 1] = std::exp(-left * dt / 2);
+    pml[n - size + i - 1] = std::exp(-right * dt / 2);
+  }
+  return pml;
+}
+
+// db2neper.m:50
+static double db2neper(double a, double y) {
+  return 100.0 * a * std::pow(1e-6 / (2 * M_PI), y) / (20.0 * std::log10(std::exp(1.0)));
+}
+
+static bool factors_235(uint64_t n) {
+  if (n == 0) return false;
+  for (uint64_t p : {2ull, 3ull, 5ull})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+// ---------------------------------------------------------------------------
+// Session
+// ---------------------------------------------------------------------------
+static std::vector<float> field_values(const kw_field& f) {
+  return std::vector<float>(f.data, f.data + f.numel);
+}
+
+template <class T>
+static T* up(DevBuf& b, const T* h, size_t n, cudaStream_t st) {
+  b.alloc(n * sizeof(T));
+  if (n) ck(cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+  return (T*)b.p;
+}
+
+void Session::check_field(const kw_field& f, const char* name, bool required) {
+  if (!f.data || f.numel == 0) {
+    if (required) throw KwError(KW_ERR_INVALID_ARGUMENT, std::string(name) + " is missing");
+    return;
+  }
+  if (f.numel != 1 && f.numel != (uint64_t)d.npts)
+    throw KwError(KW_ERR_INVALID_ARGUMENT, std::string(name) + " must be a scalar or hold Nx*Ny*Nz values");
+}
+
+Map Session::map_of(const kw_field& f, DevBuf& buf, float scalar_default) {
+  Map m{nullptr, scalar_default};
+  if (!f.data || f.numel == 0) return m;
+  if (f.numel == 1) {
+    m.s = f.data[0];
+    return m;
+  }
+  m.p = up(buf, f.data, f.numel, st);
+  return m;
+}
+
+// Sort 1-based indices, keep the last duplicate (MATLAB assignment order),
+// and return (sorted 0-based index, original position).
+static void sort_indices(const uint64_t* idx1, uint64_t n, uint64_t npts, std::vector<int>& sidx,
+                         std::vector<int>& slot, const char* name) {
+  std::vector<std::pair<long long, int>> v(n);
+  for (uint64_t j = 0; j < n; ++j) {
+    if (idx1[j] < 1 || idx1[j] > npts)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, std::string(name) + " holds an index outside the grid");
+    v[j] = {(long long)idx1[j] - 1, (int)j};
+  }
+  std::stable_sort(v.begin(), v.end(), [](auto& a, auto& b) { return a.first < b.first; });
+  sidx.clear();
+  slot.clear();
+  for (size_t j = 0; j < v.size(); ++j) {
+    if (j + 1 < v.size() && v[j + 1].first == v[j].first) continue;  // a later entry wins
+    sidx.push_back((int)v[j].first);
+    slot.push_back(v[j].second);
+  }
+}
+
+void Session::setup(const kw_input* in, const kw_options* o) {
+  if (!in || !o) throw KwError(KW_ERR_INVALID_ARGUMENT, "input and options must not be NULL");
+  opt = *o;
+  if (opt.start_index == 0) opt.start_index = 1;
+  if (in->Nx < 1 || in->Ny < 1 || in->Nz < 1 || in->Nt < 1)
+    throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
+  if (in->Ny == 1) throw KwError(KW_ERR_UNSUPPORTED, "1D simulations are not supported (Ny must be > 1)");
+  for (uint64_t n : {in->Nx, in->Ny, in->Nz}) {
+    if (n > 1 && !factors_235(n))
+      throw KwError(KW_ERR_UNSUPPORTED, "grid sizes must factor into 2, 3 and 5");
+    if (n > 4096) throw KwError(KW_ERR_UNSUPPORTED, "grid sizes above 4096 are not supported");
+  }
+  if (in->Nx < 2) throw KwError(KW_ERR_UNSUPPORTED, "Nx must be at least 2");
+  d.nx = (int)in->Nx;
+  d.ny = (int)in->Ny;
+  d.nz = (int)in->Nz;
+  d.dim = (in->Nz == 1) ? 2 : 3;
+  d.nxh = d.nx / 2 + 1;
+  d.nxp = (d.nxh + 15) / 16 * 16;
+  d.nrows = (long long)d.ny * d.nz;
+  d.npts = (long long)d.nx * d.nrows;
+  if (d.npts >= (1LL << 31)) throw KwError(KW_ERR_UNSUPPORTED, "grids above 2^31 points are not supported");
+  Nt = in->Nt;
+  if (!(in->dx > 0) || !(in->dy > 0) || (d.dim == 3 && !(in->dz > 0)) || !(in->dt > 0))
+    throw KwError(KW_ERR_INVALID_ARGUMENT, "dx, dy, (dz) and dt must be positive");
+  if (!(in->c_ref > 0)) throw KwError(KW_ERR_INVALID_ARGUMENT, "c_ref must be positive");
+  check_field(in->c0, "c0", true);
+  check_field(in->rho0, "rho0", true);
+  check_field(in->rho0_sgx, "rho0_sgx", true);
+  check_field(in->rho0_sgy, "rho0_sgy", true);
+  if (d.dim == 3) check_field(in->rho0_sgz, "rho0_sgz", true);
+  nonlinear = in->nonlinear_flag != 0;
+  if (nonlinear) check_field(in->BonA, "BonA", true);
+  eos = (int)in->absorbing_flag;
+  if (eos < 0 || eos > 2) throw KwError(KW_ERR_INVALID_ARGUMENT, "absorbing_flag must be 0, 1 or 2");
+  if (eos) check_field(in->alpha_coeff, "alpha_coeff", true);
+  if (in->p0_source_flag && !in->p0_source_input)
+    throw KwError(KW_ERR_INVALID_ARGUMENT, "p0_source_input is missing");
+  if (in->p0_source_flag && in->p_source_flag)
+    throw KwError(KW_ERR_INVALID_ARGUMENT, "p0 and p sources cannot be used together");
+
+  ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaEventCreate(&ev0), "cudaEventCreate");
+  ck(cudaEventCreate(&ev1), "cudaEventCreate");
+
+  // ----- FFT plans and twiddles (FP64 -> FP32) -----
+  const int ns[3] = {d.nx, d.ny, d.nz};
+  for (int a = 0; a < d.dim; ++a) {
+    if (!make_fft_plan(ns[a], &plan[a])) throw KwError(KW_ERR_UNSUPPORTED, "unsupported FFT size");
+    std::vector<float2> tw(ns[a]);
+    for (int k = 0; k < ns[a]; ++k) {
+      const double ang = -2.0 * M_PI * (double)k / ns[a];
+      tw[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    twd[a] = up(tw_buf[a], tw.data(), tw.size(), st);
+  }
+  col_tl[0] = 16;
+  for (int a = 1; a < d.dim; ++a) {
+    int tl = 16;
+    while (tl > 1 && (size_t)tl * ns[a] * 3 * 8 + ns[a] * 8 > 160 * 1024) tl /= 2;
+    col_tl[a] = tl;
+  }
+  rowL = std::max(1, std::min(8, 2048 / d.nx));
+
+  // ----- operator tables -----
+  const double dd[3] = {in->dx, in->dy, in->dz};
+  const double dt = in->dt, c_ref = in->c_ref;
+  for (int a = 0; a < d.dim; ++a) {
+    std::vector<double> k = kvec_fft_order(ns[a], dd[a]);
+    const int cnt = (a == 0) ? d.nxh : ns[a];
+    std::vector<float> k2(cnt);
+    std::vector<float2> pos(cnt), neg(cnt);
+    for (int b = 0; b < cnt; ++b) {
+      k2[b] = (float)(k[b] * k[b]);
+      std::complex<double> ik(0.0, k[b]);
+      std::complex<double> p = ik * std::exp(std::complex<double>(0.0, k[b] * dd[a] / 2));
+      std::complex<double> q = ik * std::exp(std::complex<double>(0.0, -k[b] * dd[a] / 2));
+      pos[b] = make_float2((float)p.real(), (float)p.imag());
+      neg[b] = make_float2((float)q.real(), (float)q.imag());
+    }
+    T.k2[a] = up(k2_buf[a], k2.data(), cnt, st);
+    T.ddk_pos[a] = up(pos_buf[a], pos.data(), cnt, st);
+    T.ddk_neg[a] = up(neg_buf[a], neg.data(), cnt, st);
+    const uint64_t psz[3] = {in->pml_x_size, in->pml_y_size, in->pml_z_size};
+    const double pal[3] = {in->pml_x_alpha, in->pml_y_alpha, in->pml_z_alpha};
+    if (psz[a] * 2 > (uint64_t)ns[a]) throw KwError(KW_ERR_INVALID_ARGUMENT, "PML is larger than the grid");
+    std::vector<double> pm = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], false);
+    std::vector<double> pms = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], true);
+    std::vector<float> f1(pm.begin(), pm.end()), f2(pms.begin(), pms.end());
+    pml_d[a] = up(pml_buf[a], f1.data(), f1.size(), st);
+    pml_sg_d[a] = up(pmls_buf[a], f2.data(), f2.size(), st);
+  }
+  if (d.dim == 2) {
+    T.k2[2] = T.k2[1];
+    T.ddk_pos[2] = T.ddk_pos[1];
+    T.ddk_neg[2] = T.ddk_neg[1];
+  }
+  T.cdt2 = (float)(c_ref * dt / 2.0);
+  T.scale = (float)(1.0 / (double)d.npts);
+  T.ym2 = (float)(in->alpha_power - 2.0);
+  T.ym1 = (float)(in->alpha_power - 1.0);
+  dtf = in->dt;
+
+  // ----- medium -----
+  {
+    std::vector<float> c0 = field_values(in->c0);
+    std::vector<float> c0sq(c0.size());
+    for (size_t i = 0; i < c0.size(); ++i) c0sq[i] = c0[i] * c0[i];
+    kw_field f{c0sq.data(), (uint64_t)c0sq.size()};
+    c0sq_m = map_of(f, c0sq_buf, 0.f);
+    rho0_m = map_of(in->rho0, rho0_buf, 0.f);
+    const kw_field* sg[3] = {&in->rho0_sgx, &in->rho0_sgy, &in->rho0_sgz};
+    for (int a = 0; a < d.dim; ++a) {
+      std::vector<float> v = field_values(*sg[a]);
+      for (auto& x : v) x = 1.0f / x;
+      kw_field g{v.data(), (uint64_t)v.size()};
+      rinv_m[a] = map_of(g, rinv_buf[a], 0.f);
+    }
+    if (nonlinear) bona_m = map_of(in->BonA, bona_buf, 0.f);
+    if (eos == 1 || eos == 2) {
+      const bool het = in->c0.numel > 1 || in->alpha_coeff.numel > 1;
+      const size_t n = het ? (size_t)d.npts : 1;
+      const double y = in->alpha_power;
+      std::vector<float> ctau(n), ceta(n);
+      for (size_t i = 0; i < n; ++i) {
+        const double c = in->c0.numel > 1 ? (double)in->c0.data[i] : (double)in->c0.data[0];
+        const double al = in->alpha_coeff.numel > 1 ? (double)in->alpha_coeff.data[i] : (double)in->alpha_coeff.data[0];
+        const double csq = (double)((float)c * (float)c);
+        if (eos == 1) {
+          const double a = db2neper(al, y);
+          const double tau = -2.0 * a * std::pow(c, y - 1.0);
+          const double eta = 2.0 * a * std::pow(c, y) * std::tan(M_PI * y / 2.0);
+          ctau[i] = (float)(csq * (double)(float)tau);
+          ceta[i] = (float)(csq * (double)(float)eta);
+        } else {
+          const double a = db2neper(al, 2.0);
+          ctau[i] = (float)(-2.0 * a * c);  // stokes: tau itself
+        }
+      }
+      kw_field ft{ctau.data(), (uint64_t)n}, fe{ceta.data(), (uint64_t)n};
+      if (eos == 1) {
+        c2tau_m = map_of(ft, c2tau_buf, 0.f);
+        c2eta_m = map_of(fe, c2eta_buf, 0.f);
+      } else {
+        tau_m = map_of(ft, c2tau_buf, 0.f);
+      }
+    }
+  }
+
+  // ----- fields and spectral work buffers -----
+  const size_t fb = sizeof(float) * d.npts;
+  const size_t sb = sizeof(float2) * (size_t)d.nxp * d.nrows;
+  for (int a = 0; a < d.dim; ++a) {
+    u_buf[a].alloc(fb);
+    rho_buf[a].alloc(fb);
+    ck(cudaMemsetAsync(u_buf[a].p, 0, fb, st), "memset");
+    ck(cudaMemsetAsync(rho_buf[a].p, 0, fb, st), "memset");
+  }
+  for (int s = 0; s < 4; ++s) {
+    S_buf[s].alloc(sb);
+    ck(cudaMemsetAsync(S_buf[s].p, 0, sb, st), "memset");
+  }
+  if (eos == 1) ploc_buf.alloc(fb);
+  if (opt.p_final) {
+    p_buf.alloc(fb);
+    ck(cudaMemsetAsync(p_buf.p, 0, fb, st), "memset");
+  }
+  int one = 1;
+  clock_buf.alloc(sizeof(int));
+  ck(cudaMemcpyAsync(clock_buf.p, &one, sizeof(int), cudaMemcpyHostToDevice, st), "clock");
+  clk.t = (const int*)clock_buf.p;
+  clk.start = (int)opt.start_index;
+
+  // ----- sources -----
+  p0 = in->p0_source_flag != 0;
+  if (p0) up(p0_buf, in->p0_source_input, (size_t)d.npts, st);
+  setup_sources(in);
+
+  // ----- sensors -----
+  setup_sensors(in);
+  ck(cudaStreamSynchronize(st), "setup");
+}
+
+void Session::setup_sources(const kw_input* in) {
+  psrc = SparseSource{};
+  pdense = DenseSource{};
+  if (in->p_source_flag) {
+    if (!in->p_source_index || !in->p_source_input || in->p_source_index_numel == 0)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "p_source_index / p_source_input missing");
+    std::vector<int> si, sl;
+    sort_indices(in->p_source_index, in->p_source_index_numel, d.npts, si, sl, "p_source_index");
+    const int nsig = in->p_source_many ? (int)in->p_source_index_numel : 1;
+    p_mode = (int)in->p_source_mode;
+    if (p_mode < 0 || p_mode > 2) throw KwError(KW_ERR_INVALID_ARGUMENT, "p_source_mode must be 0, 1 or 2");
+    p_len = (int)in->p_source_flag;
+    const int* didx = up(psrc_idx, si.data(), si.size(), st);
+    const int* dslot = up(psrc_slot, sl.data(), sl.size(), st);
+    const float* dsig = up(psrc_sig, in->p_source_input, (size_t)nsig * p_len, st);
+    p_nsrc = (int)si.size();
+    p_nsig = nsig;
+    if (p_mode == 2) {
+      pdense.len = p_len;
+      if (nsig == 1) {
+        // single signal: the corrected field is sig(t) * F^-1{cos(.) F{mask}}
+        psrc_field.alloc(sizeof(float) * d.npts);
+        std::vector<float> ones(1, 1.0f);
+        DevBuf onebuf;
+        const float* d1 = up(onebuf, ones.data(), 1, st);
+        corrected_source((float*)psrc_field.p, didx, dslot, p_nsrc, d1, 1, 1);
+        ck(cudaStreamSynchronize(st), "source setup");
+        pdense.field = (const float*)psrc_field.p;
+        pdense.sig = dsig;
+      } else {
+        psrc_field.alloc(sizeof(float) * d.npts);
+        pdense.field = (const float*)psrc_field.p;
+        pdense.sig = nullptr;
+        p_many_additive = true;
+      }
+    } else {
+      psrc.n = p_nsrc;
+      psrc.idx = didx;
+      psrc.slot = dslot;
+      psrc.sig = dsig;
+      psrc.nrows_sig = nsig;
+      psrc.len = p_len;
+      psrc.mode = p_mode;  // 0 dirichlet, 1 add
+    }
+  }
+  usrc = SparseSource{};
+  for (int a = 0; a < 3; ++a) {
+    udense[a] = DenseSource{};
+    usig_d[a] = nullptr;
+    u_len[a] = 0;
+  }
+  const uint64_t uf[3] = {in->ux_source_flag, in->uy_source_flag, in->uz_source_flag};
+  const float* uin[3] = {in->ux_source_input, in->uy_source_input, in->uz_source_input};
+  if (uf[0] || uf[1] || (d.dim == 3 && uf[2])) {
+    if (!in->u_source_index || in->u_source_index_numel == 0)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "u_source_index missing");
+    std::vector<int> si, sl;
+    sort_indices(in->u_source_index, in->u_source_index_numel, d.npts, si, sl, "u_source_index");
+    const int nsig = in->u_source_many ? (int)in->u_source_index_numel : 1;
+    u_mode = (int)in->u_source_mode;
+    if (u_mode < 0 || u_mode > 2) throw KwError(KW_ERR_INVALID_ARGUMENT, "u_source_mode must be 0, 1 or 2");
+    const int* didx = up(usrc_idx, si.data(), si.size(), st);
+    const int* dslot = up(usrc_slot, sl.data(), sl.size(), st);
+    u_nsrc = (int)si.size();
+    u_nsig = nsig;
+    for (int a = 0; a < d.dim; ++a) {
+      if (!uf[a]) continue;
+      if (!uin[a]) throw KwError(KW_ERR_INVALID_ARGUMENT, "velocity source input missing");
+      u_len[a] = (int)uf[a];
+      usig_d[a] = up(usig_buf[a], uin[a], (size_t)nsig * u_len[a], st);
+    }
+    if (u_mode == 2) {
+      for (int a = 0; a < d.dim; ++a) {
+        if (!uf[a]) continue;
+        udense[a].len = u_len[a];
+        ufield_buf[a].alloc(sizeof(float) * d.npts);
+        udense[a].field = (const float*)ufield_buf[a].p;
+        if (nsig == 1) {
+          if (!ones_ready) {
+            std::vector<float> ones(1, 1.0f);
+            const float* d1 = up(ones_buf, ones.data(), 1, st);
+            corrected_source((float*)ufield_buf[a].p, didx, dslot, u_nsrc, d1, 1, 1);
+            ones_ready = true;
+            ones_field = a;
+          } else {
+            ck(cudaMemcpyAsync(ufield_buf[a].p, ufield_buf[ones_field].p, sizeof(float) * d.npts,
+                               cudaMemcpyDeviceToDevice, st), "copy");
+          }
+          udense[a].sig = usig_d[a];
+        } else {
+          udense[a].sig = nullptr;
+          u_many_additive = true;
+        }
+      }
+    } else {
+      usrc.n = u_nsrc;
+      usrc.idx = didx;
+      usrc.slot = dslot;
+      usrc.nrows_sig = nsig;
+      usrc.mode = u_mode;
+      usrc.len = 0;
+    }
+  }
+}
+
+// out = real(ifftn(source_kappa .* fftn(scatter(sig(:, t)))))
+// (kspaceFirstOrder3D.m:813-821, 938-945)
+void Session::corrected_source(float* out, const int* idx, const int* slot, int n, const float* sig,
+                               int nrows_sig, int t) {
+  ck(cudaMemsetAsync(out, 0, sizeof(float) * d.npts, st), "memset");
+  ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, st), "scatter");
+  float2* S = (float2*)S_buf[3].p;
+  ck(launch_x_r2c(out, S, d, plan[0], twd[0], rowL, st), "x_r2c");
+  run_spectral({S}, {S}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
+  ck(launch_x_c2r(S, out, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
+}
+
+// y passes (3D) around the fused last-axis operator.  `ins` are x-transformed
+// half spectra; outputs are left x-transformed (ready for the row kernels).
+void Session::run_spectral(std::vector<float2*> ins, std::vector<float2*> outs, std::vector<SpecOp> ops,
+                           int fanout) {
+  const int nin = (int)ins.size();
+  if (d.dim == 3) {
+    ColArgs ca{};
+    for (int i = 0; i < nin; ++i) ca.buf[i] = ins[i];
+    ca.ncols = d.nxh;
+    ca.lstride = d.nxp;
+    ca.ostride = (long long)d.nxp * d.ny;
+    ca.tl = col_tl[1];
+    ck(launch_col_fft(false, ca, nin, d.nz, plan[1], twd[1], st), "col_fft fwd");
+    ++launches_;
+  }
+  const int last = d.dim - 1;
+  FusedArgs fa{};
+  for (int i = 0; i < nin; ++i) fa.in[i] = ins[i];
+  for (size_t i = 0; i < outs.size(); ++i) {
+    fa.out[i] = outs[i];
+    fa.op[i] = ops[i];
+  }
+  fa.fanout = fanout;
+  fa.ncols = d.nxh;
+  fa.lstride = (long long)d.nxp * (d.dim == 3 ? d.ny : 1);
+  fa.ostride = d.nxp;
+  fa.tl = col_tl[last];
+  ck(launch_fused_last(fa, nin, d.dim == 3 ? d.ny : 1, plan[last], twd[last], T, d.dim, st), "fused_last");
+  ++launches_;
+  if (d.dim == 3) {
+    ColArgs ca{};
+    for (size_t i = 0; i < outs.size(); ++i) ca.buf[i] = outs[i];
+    ca.ncols = d.nxh;
+    ca.lstride = d.nxp;
+    ca.ostride = (long long)d.nxp * d.ny;
+    ca.tl = col_tl[1];
+    ck(launch_col_fft(true, ca, (int)outs.size(), d.nz, plan[1], twd[1], st), "col_fft inv");
+    ++launches_;
+  }
+}
+
+void Session::setup_sensors(const kw_input* in) {
+  std::vector<int> si, sl;
+  if (in->sensor_mask_type == 0) {
+    if (!in->sensor_mask_index || in->sensor_mask_index_numel == 0)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_index missing");
+    ns = (long long)in->sensor_mask_index_numel;
+    std::vector<uint64_t> lin(in->sensor_mask_index, in->sensor_mask_index + ns);
+    build_sensor_lists(lin, si, sl);
+  } else if (in->sensor_mask_type == 1) {
+    if (!in->sensor_mask_corners || in->sensor_mask_corners_numel == 0 || in->sensor_mask_corners_numel % 6)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_corners must hold 6 values per cuboid");
+    std::vector<uint64_t> lin;
+    const uint64_t K = in->sensor_mask_corners_numel / 6;
+    for (uint64_t k = 0; k < K; ++k) {
+      const uint64_t* c = in->sensor_mask_corners + 6 * k;
+      const uint64_t lim[3] = {(uint64_t)d.nx, (uint64_t)d.ny, (uint64_t)d.nz};
+      for (int a = 0; a < 3; ++a)
+        if (c[a] < 1 || c[a + 3] < c[a] || c[a + 3] > lim[a])
+          throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_corners outside the grid or not ordered");
+      // concatenated find() per cuboid (kspaceFirstOrder_inputChecking.m:1615-1636)
+      for (uint64_t z = c[2]; z <= c[5]; ++z)
+        for (uint64_t y = c[1]; y <= c[4]; ++y)
+          for (uint64_t x = c[0]; x <= c[3]; ++x)
+            lin.push_back((x - 1) + (uint64_t)d.nx * ((y - 1) + (uint64_t)d.ny * (z - 1)) + 1);
+    }
+    ns = (long long)lin.size();
+    build_sensor_lists(lin, si, sl);
+  } else {
+    throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_type must be 0 or 1");
+  }
+  if (opt.start_index > Nt) nrec = 0;
+  else nrec = (long long)(Nt - opt.start_index + 1);
+  // sensor state for p and u
+  auto mk = [&](Sensor& s) {
+    s = Sensor{};
+    s.mode = dense_sensor ? 1 : 2;
+    s.ns = (int)ns;
+    s.idx = dense_sensor ? nullptr : sidx_d;
+    s.slot = dense_sensor ? nullptr : sslot_d;
+  };
+  mk(sens_p);
+  const size_t ser = sizeof(float) * (size_t)ns * (size_t)nrec;
+  const size_t per = sizeof(float) * (size_t)ns;
+  const size_t all = sizeof(float) * (size_t)d.npts;
+  auto zalloc = [&](DevBuf& b, size_t n) -> void* {
+    b.alloc(n);
+    if (n) ck(cudaMemsetAsync(b.p, 0, n, st), "memset");
+    return b.p;
+  };
+  if (opt.p_raw && nrec) sens_p.raw = (float*)zalloc(p_raw_buf, ser);
+  if (opt.p_max) sens_p.vmax = (float*)zalloc(p_max_buf, per);
+  if (opt.p_min) sens_p.vmin = (float*)zalloc(p_min_buf, per);
+  if (opt.p_rms) {
+    sens_p.rms = (float2*)zalloc(p_rms_buf, 2 * per);
+    zalloc(p_rmsf_buf, per);
+  }
+  if (opt.p_max_all) sens_p.max_all = (float*)zalloc(p_maxall_buf, all);
+  if (opt.p_min_all) sens_p.min_all = (float*)zalloc(p_minall_buf, all);
+  for (int a = 0; a < d.dim; ++a) {
+    mk(sens_u[a]);
+    if (opt.u_raw && nrec) sens_u[a].raw = (float*)zalloc(u_raw_buf[a], ser);
+    if (opt.u_max) sens_u[a].vmax = (float*)zalloc(u_max_buf[a], per);
+    if (opt.u_min) sens_u[a].vmin = (float*)zalloc(u_min_buf[a], per);
+    if (opt.u_rms) {
+      sens_u[a].rms = (float2*)zalloc(u_rms_buf[a], 2 * per);
+      zalloc(u_rmsf_buf[a], per);
+    }
+    if (opt.u_max_all) sens_u[a].max_all = (float*)zalloc(u_maxall_buf[a], all);
+    if (opt.u_min_all) sens_u[a].min_all = (float*)zalloc(u_minall_buf[a], all);
+    const bool any = sens_u[a].raw || sens_u[a].vmax || sens_u[a].vmin || sens_u[a].rms ||
+                     sens_u[a].max_all || sens_u[a].min_all;
+    if (!any) sens_u[a].mode = 0;
+  }
+  {
+    const bool any = sens_p.raw || sens_p.vmax || sens_p.vmin || sens_p.rms || sens_p.max_all || sens_p.min_all;
+    if (!any) sens_p.mode = 0;
+  }
+  if (opt.u_non_staggered_raw)
+    throw KwError(KW_ERR_UNSUPPORTED, "u_non_staggered_raw is not supported yet");
+}
+
+void Session::build_sensor_lists(const std::vector<uint64_t>& lin, std::vector<int>& si, std::vector<int>& sl) {
+  // dense identity: every grid point in linear order
+  dense_sensor = ((long long)lin.size() == d.npts);
+  if (dense_sensor)
+    for (long long j = 0; j < d.npts; ++j)
+      if (lin[j] != (uint64_t)j + 1) {
+        dense_sensor = false;
+        break;
+      }
+  if (dense_sensor) return;
+  std::vector<std::pair<long long, int>> v(lin.size());
+  for (size_t j = 0; j < lin.size(); ++j) {
+    if (lin[j] < 1 || lin[j] > (uint64_t)d.npts)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_index holds an index outside the grid");
+    v[j] = {(long long)lin[j] - 1, (int)j};
+  }
+  std::stable_sort(v.begin(), v.end(), [](auto& a, auto& b) { return a.first < b.first; });
+  si.resize(v.size());
+  sl.resize(v.size());
+  for (size_t j = 0; j < v.size(); ++j) {
+    si[j] = (int)v[j].first;
+    sl[j] = v[j].second;
+  }
+  sidx_d = up(sidx_buf, si.data(), si.size(), st);
+  sslot_d = up(sslot_buf, sl.data(), sl.size(), st);
+}
+
+// t = 1 with an initial pressure (kspaceFirstOrder3D.m:1021-1035):
+// p = p0, rho_i = p0 / (dim c0^2), u_i = dt rho0_sg_inv grad_i(p0) / 2.
+void Session::enqueue_init() {
+  const float* p0d = (const float*)p0_buf.p;
+  ck(launch_record_field(p0d, sens_p, clk, d.npts, st), "record p0");
+  ++launches_;
+  ck(launch_rho_init((float*)rho_buf[0].p, (float*)rho_buf[1].p, d.dim == 3 ? (float*)rho_buf[2].p : nullptr,
+                     p0d, c0sq_m, d.dim, d.npts, st), "rho init");
+  ++launches_;
+  float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
+  ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
+  ++launches_;
+  std::vector<float2*> outs;
+  std::vector<SpecOp> ops;
+  for (int a = 0; a < d.dim; ++a) {
+    outs.push_back(S[a + 1]);
+    ops.push_back(SpecOp{OP_GRAD_POS, a});
+  }
+  run_spectral({S[0]}, outs, ops, d.dim);
+  UArgs ua = u_args(S);
+  ua.init = 1;
+  ua.do_r2c = 0;
+  ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u init");
+  ++launches_;
+  ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
+  ++launches_;
+  if (p_buf.p)
+    ck(cudaMemcpyAsync(p_buf.p, p0d, sizeof(float) * d.npts, cudaMemcpyDeviceToDevice, st), "p0 copy");
+}
+
+UArgs Session::u_args(float2* const* S) {
+  UArgs ua{};
+  for (int a = 0; a < d.dim; ++a) {
+    ua.S[a] = S[a + 1];
+    ua.Sout[a] = S[a + 1];
+    ua.u[a] = (float*)u_buf[a].p;
+    ua.rinv[a] = rinv_m[a];
+    ua.pml_sg[a] = pml_sg_d[a];
+    ua.src_sig[a] = usig_d[a];
+    ua.src_len[a] = u_len[a];
+    ua.dsrc[a] = udense[a];
+    ua.sens[a] = sens_u[a];
+  }
+  ua.dt = dtf;
+  ua.init = 0;
+  ua.do_r2c = 1;
+  ua.src = usrc;
+  ua.clk = clk;
+  return ua;
+}
+
+void Session::enqueue_step() {
+  const uint64_t t = t_done + 1;
+  if (t == 1 && p0) {
+    enqueue_init();
+  } else {
+    float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
+    // (1) momentum: grad p -> u (kspaceFirstOrder3D.m:790-884)
+    std::vector<float2*> outs;
+    std::vector<SpecOp> ops;
+    for (int a = 0; a < d.dim; ++a) {
+      outs.push_back(S[a + 1]);
+      ops.push_back(SpecOp{OP_GRAD_POS, a});
+    }
+    run_spectral({S[0]}, outs, ops, d.dim);
+    if (u_many_additive) {
+      for (int a = 0; a < d.dim; ++a)
+        if (udense[a].field && (int)t <= u_len[a]) {
+          // S[0] is free here: the gradient has been taken
+          corrected_source_into((float*)ufield_buf[a].p, (const int*)usrc_idx.p, (const int*)usrc_slot.p, u_nsrc,
+                                usig_d[a], u_nsig, (int)t, S[0]);
+        }
+    }
+    UArgs ua = u_args(S);
+    ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u");
+    ++launches_;
+    // (2) mass conservation: div u -> rho, EOS (:905-1017)
+    std::vector<float2*> ins2, outs2;
+    std::vector<SpecOp> ops2;
+    for (int a = 0; a < d.dim; ++a) {
+      ins2.push_back(S[a + 1]);
+      outs2.push_back(S[a + 1]);
+      ops2.push_back(SpecOp{OP_GRAD_NEG, a});
+    }
+    run_spectral(ins2, outs2, ops2, 1);
+    if (p_many_additive && (int)t <= p_len)
+      corrected_source_into((float*)psrc_field.p, (const int*)psrc_idx.p, (const int*)psrc_slot.p, p_nsrc,
+                            (const float*)psrc_sig.p, p_nsig, (int)t, S[0]);
+    RhoArgs ra{};
+    for (int a = 0; a < d.dim; ++a) {
+      ra.S[a] = S[a + 1];
+      ra.rho[a] = (float*)rho_buf[a].p;
+      ra.pml[a] = pml_d[a];
+    }
+    ra.rho0 = rho0_m;
+    ra.dt = dtf;
+    ra.nonlinear = nonlinear;
+    ra.bona = bona_m;
+    ra.c0sq = c0sq_m;
+    ra.eos = eos;
+    ra.tau = tau_m;
+    ra.src = psrc;
+    ra.dsrc = pdense;
+    ra.sens = sens_p;
+    ra.clk = clk;
+    const bool last = (t == Nt);
+    if (eos == 1) {
+      ra.p_loc = (float*)ploc_buf.p;
+      ra.S_q = S[1];
+      ra.S_r = S[2];
+    } else {
+      ra.p_out = last ? (float*)p_buf.p : nullptr;
+      ra.S_p = S[0];
+    }
+    ck(launch_x_rho(ra, d, plan[0], twd[0], rowL, st), "x_rho");
+    ++launches_;
+    if (eos == 1) {
+      // (3) power-law absorption and dispersion (:970-977)
+      run_spectral({S[1], S[2]}, {S[1], S[2]}, {SpecOp{OP_NABLA1, 0}, SpecOp{OP_NABLA2, 0}}, 1);
+      EosArgs ea{};
+      ea.S_a = S[1];
+      ea.S_b = S[2];
+      ea.p_loc = (const float*)ploc_buf.p;
+      ea.c2tau = c2tau_m;
+      ea.c2eta = c2eta_m;
+      ea.p_out = last ? (float*)p_buf.p : nullptr;
+      ea.S_p = S[0];
+      ea.sens = sens_p;
+      ea.clk = clk;
+      ck(launch_x_eos(ea, d, plan[0], twd[0], rowL, st), "x_eos");
+      ++launches_;
+    }
+  }
+  ck(launch_advance((int*)clock_buf.p, st), "advance");
+  ++launches_;
+  ++t_done;
+}
+
+// corrected source field for "many" signals, using `work` as spectral scratch
+void Session::corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
+                                    int nrows_sig, int t, float2* work) {
+  ck(cudaMemsetAsync(out, 0, sizeof(float) * d.npts, st), "memset");
+  ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, st), "scatter");
+  ck(launch_x_r2c(out, work, d, plan[0], twd[0], rowL, st), "x_r2c");
+  run_spectral({work}, {work}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
+  ck(launch_x_c2r(work, out, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
+  launches_ += 4;
+}
+
+void Session::advance(uint64_t n) {
+  if (t_done + n > Nt) throw KwError(KW_ERR_INVALID_ARGUMENT, "advance beyond Nt");
+  ck(cudaEventRecord(ev0, st), "event");
+  const uint64_t l0 = launches_;
+  for (uint64_t i = 0; i < n; ++i) enqueue_step();
+  last_launches = launches_ - l0;
+  last_steps = n;
+  ck(cudaEventRecord(ev1, st), "event");
+}
+
+float Session::elapsed_ms() {
+  ck(cudaEventSynchronize(ev1), "event sync");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, ev0, ev1), "elapsed");
+  return ms;
+}
+
+void Session::sync() { ck(cudaStreamSynchronize(st), "sync"); }
+
+static void d2h(float* dst, const void* src, size_t n, cudaStream_t st) {
+  if (dst && src && n) ck(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost, st), "d2h");
+}
+
+void Session::read(kw_output* out) {
+  if (!out) throw KwError(KW_ERR_INVALID_ARGUMENT, "output must not be NULL");
+  const long long nr = std::min<long long>(nrec, std::max<long long>(0, (long long)t_done - (long long)opt.start_index + 1));
+  const float inv = nr > 0 ? 1.0f / (float)nr : 0.f;
+  if (p_rms_buf.p) ck(launch_rms_final((const float2*)p_rms_buf.p, (float*)p_rmsf_buf.p, ns, inv, st), "rms");
+  for (int a = 0; a < d.dim; ++a)
+    if (u_rms_buf[a].p) ck(launch_rms_final((const float2*)u_rms_buf[a].p, (float*)u_rmsf_buf[a].p, ns, inv, st), "rms");
+  const size_t ser = (size_t)ns * (size_t)nrec, per = (size_t)ns, all = (size_t)d.npts;
+  d2h(out->p, p_raw_buf.p, ser, st);
+  d2h(out->p_max, p_max_buf.p, per, st);
+  d2h(out->p_min, p_min_buf.p, per, st);
+  d2h(out->p_rms, p_rmsf_buf.p, per, st);
+  d2h(out->p_max_all, p_maxall_buf.p, all, st);
+  d2h(out->p_min_all, p_minall_buf.p, all, st);
+  d2h(out->p_final, p_buf.p, all, st);
+  float* ur[3] = {out->ux, out->uy, out->uz};
+  float* umx[3] = {out->ux_max, out->uy_max, out->uz_max};
+  float* umn[3] = {out->ux_min, out->uy_min, out->uz_min};
+  float* urm[3] = {out->ux_rms, out->uy_rms, out->uz_rms};
+  float* uma[3] = {out->ux_max_all, out->uy_max_all, out->uz_max_all};
+  float* umi[3] = {out->ux_min_all, out->uy_min_all, out->uz_min_all};
+  float* ufi[3] = {out->ux_final, out->uy_final, out->uz_final};
+  for (int a = 0; a < d.dim; ++a) {
+    d2h(ur[a], u_raw_buf[a].p, ser, st);
+    d2h(umx[a], u_max_buf[a].p, per, st);
+    d2h(umn[a], u_min_buf[a].p, per, st);
+    d2h(urm[a], u_rmsf_buf[a].p, per, st);
+    d2h(uma[a], u_maxall_buf[a].p, all, st);
+    d2h(umi[a], u_minall_buf[a].p, all, st);
+    if (opt.u_final) d2h(ufi[a], u_buf[a].p, all, st);
+  }
+  sync();
+}
+
+Session::~Session() {
+  if (st) cudaStreamSynchronize(st);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (st) cudaStreamDestroy(st);
+}
+
+size_t Session::device_bytes_estimate(const kw_input* in, const kw_options* o) {
+  const size_t n = (size_t)(in->Nx * in->Ny * in->Nz);
+  const size_t dim = in->Nz == 1 ? 2 : 3;
+  const size_t nxp = ((in->Nx / 2 + 1) + 15) / 16 * 16;
+  size_t b = 4 * 8 * nxp * in->Ny * in->Nz + 2 * dim * 4 * n;  // spectra, u, rho
+  b += 4 * n * (2 + dim);                                       // medium maps
+  return b;
+}
+
+}  // namespace kwb
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using kwb::KwError;
+using kwb::Session;
+
+struct kw_session {
+  std::unique_ptr<Session> s;
+};
+
+static int set_status(kw_status* st, int code, const std::string& msg) {
+  if (st) {
+    st->code = code;
+    std::snprintf(st->message, sizeof(st->message), "%s", msg.c_str());
+  }
+  return code;
+}
+
+template <class F>
+static int guarded(kw_status* st, F&& f) {
+  try {
+    f();
+    return set_status(st, KW_OK, "");
+  } catch (const KwError& e) {
+    return set_status(st, e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return set_status(st, KW_ERR_OUT_OF_MEMORY, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_status(st, KW_ERR_INTERNAL, e.what());
+  }
+}
+
+static void select_device(const kw_options* opt) {
+  if (opt && opt->device >= 0) {
+    cudaError_t e = cudaSetDevice(opt->device);
+    if (e != cudaSuccess) throw KwError(KW_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  }
+}
+
+extern "C" {
+
+const char* kw_version(void) { return "kwave_b200 0.1.0 (sm_100a)"; }
+
+int kw_output_sizes_query(const kw_input* in, const kw_options* opt, kw_output_sizes* sizes, kw_status* status) {
+  return guarded(status, [&] {
+    if (!in || !opt || !sizes) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (in->Nx < 1 || in->Ny < 1 || in->Nz < 1 || in->Nt < 1)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
+    uint64_t nsens = 0;
+    if (in->sensor_mask_type == 0) {
+      nsens = in->sensor_mask_index_numel;
+    } else if (in->sensor_mask_type == 1) {
+      if (!in->sensor_mask_corners || in->sensor_mask_corners_numel % 6)
+        throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_corners must hold 6 values per cuboid");
+      for (uint64_t k = 0; k < in->sensor_mask_corners_numel / 6; ++k) {
+        const uint64_t* c = in->sensor_mask_corners + 6 * k;
+        uint64_t m = 1;
+        for (int a = 0; a < 3; ++a) {
+          if (c[a + 3] < c[a]) throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_corners not ordered");
+          m *= c[a + 3] - c[a] + 1;
+        }
+        nsens += m;
+      }
+    } else {
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_type must be 0 or 1");
+    }
+    const uint64_t s = opt->start_index ? opt->start_index : 1;
+    sizes->num_sensor_points = nsens;
+    sizes->num_recorded_steps = (s > in->Nt) ? 0 : in->Nt - s + 1;
+    sizes->grid_points = in->Nx * in->Ny * in->Nz;
+    sizes->device_bytes = Session::device_bytes_estimate(in, opt);
+  });
+}
+
+int kw_session_create(const kw_input* in, const kw_options* opt, kw_session** session, kw_status* status) {
+  return guarded(status, [&] {
+    if (!session) throw KwError(KW_ERR_INVALID_ARGUMENT, "session must not be NULL");
+    *session = nullptr;
+    select_device(opt);
+    auto h = std::make_unique<kw_session>();
+    h->s = std::make_unique<Session>();
+    h->s->setup(in, opt);
+    *session = h.release();
+  });
+}
+
+int kw_session_advance(kw_session* s, uint64_t nsteps, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL session");
+    s->s->advance(nsteps);
+  });
+}
+
+int kw_session_elapsed_ms(kw_session* s, float* ms, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s || !ms) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL argument");
+    *ms = s->s->elapsed_ms();
+  });
+}
+
+int kw_session_sync(kw_session* s, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL session");
+    s->s->sync();
+  });
+}
+
+uint64_t kw_session_steps_done(const kw_session* s) { return s ? s->s->t_done : 0; }
+
+int kw_session_read(kw_session* s, kw_output* out, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL session");
+    s->s->read(out);
+  });
+}
+
+void* kw_session_stream(kw_session* s) { return s ? (void*)s->s->st : nullptr; }
+
+uint64_t kw_session_launches_per_step(const kw_session* s) { return s ? s->s->last_launches_per_step() : 0; }
+
+void kw_session_destroy(kw_session* s) { delete s; }
+
+int kw_solve(const kw_input* in, const kw_options* opt, kw_output* out, kw_status* status) {
+  return guarded(status, [&] {
+    select_device(opt);
+    Session s;
+    s.setup(in, opt);
+    s.advance(s.Nt);
+    s.read(out);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// Internal host-side types of the solver (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "kwave_b200.h"
+
+namespace kwb {
+
+struct KwError : std::runtime_error {
+  int code;
+  KwError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Owning device allocation.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf();
+  void alloc(size_t nbytes);
+};
+
+class Session {
+ public:
+  ~Session();
+  void setup(const kw_input* in, const kw_options* opt);
+  void advance(uint64_t n);
+  float elapsed_ms();
+  void sync();
+  void read(kw_output* out);
+  uint64_t last_launches_per_step() const { return last_steps ? last_launches / last_steps : 0; }
+  static size_t device_bytes_estimate(const kw_input* in, const kw_options* opt);
+
+  cudaStream_t st = nullptr;
+  uint64_t Nt = 0;
+  uint64_t t_done = 0;
+
+ private:
+  void check_field(const kw_field& f, const char* name, bool required);
+  Map map_of(const kw_field& f, DevBuf& buf, float scalar_default);
+  void setup_sources(const kw_input* in);
+  void setup_sensors(const kw_input* in);
+  void build_sensor_lists(const std::vector<uint64_t>& lin, std::vector<int>& si, std::vector<int>& sl);
+  void corrected_source(float* out, const int* idx, const int* slot, int n, const float* sig, int nrows_sig,
+                        int t);
+  void corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
+                             int nrows_sig, int t, float2* work);
+  void run_spectral(std::vector<float2*> ins, std::vector<float2*> outs, std::vector<SpecOp> ops, int fanout);
+  void enqueue_init();
+  void enqueue_step();
+  UArgs u_args(float2* const* S);
+
+  kw_options opt{};
+  Dims d{};
+  FFTPlan plan[3]{};
+  const float2* twd[3]{};
+  int col_tl[3]{16, 16, 16};
+  int rowL = 8;
+  SpecTables T{};
+  float dtf = 0.f;
+  bool nonlinear = false;
+  int eos = 0;
+  bool p0 = false;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint64_t launches_ = 0, last_launches = 0, last_steps = 0;
+
+  // operator tables
+  DevBuf tw_buf[3], k2_buf[3], pos_buf[3], neg_buf[3], pml_buf[3], pmls_buf[3];
+  const float* pml_d[3]{};
+  const float* pml_sg_d[3]{};
+  // medium
+  DevBuf c0sq_buf, rho0_buf, rinv_buf[3], bona_buf, c2tau_buf, c2eta_buf;
+  Map c0sq_m{}, rho0_m{}, rinv_m[3]{}, bona_m{}, c2tau_m{}, c2eta_m{}, tau_m{};
+  // fields
+  DevBuf u_buf[3], rho_buf[3], S_buf[4], ploc_buf, p_buf, p0_buf, clock_buf;
+  Clock clk{};
+  // sources
+  SparseSource psrc{}, usrc{};
+  DenseSource pdense{}, udense[3]{};
+  DevBuf psrc_idx, psrc_slot, psrc_sig, psrc_field;
+  DevBuf usrc_idx, usrc_slot, usig_buf[3], ufield_buf[3], ones_buf;
+  const float* usig_d[3]{};
+  int u_len[3]{};
+  int p_mode = 0, p_len = 0, p_nsrc = 0, p_nsig = 1;
+  int u_mode = 0, u_nsrc = 0, u_nsig = 1;
+  bool p_many_additive = false, u_many_additive = false, ones_ready = false;
+  int ones_field = 0;
+  // sensors
+  long long ns = 0, nrec = 0;
+  bool dense_sensor = false;
+  DevBuf sidx_buf, sslot_buf;
+  const int* sidx_d = nullptr;
+  const int* sslot_d = nullptr;
+  Sensor sens_p{}, sens_u[3]{};
+  DevBuf p_raw_buf, p_max_buf, p_min_buf, p_rms_buf, p_rmsf_buf, p_maxall_buf, p_minall_buf;
+  DevBuf u_raw_buf[3], u_max_buf[3], u_min_buf[3], u_rms_buf[3], u_rmsf_buf[3], u_maxall_buf[3], u_minall_buf[3];
+};
+
+}  // namespace kwb

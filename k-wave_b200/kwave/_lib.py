@@ -1,0 +1,377 @@
+"""ctypes binding of ``include/kwave_b200.h``.
+
+The structures mirror the C declarations field by field.  ``solve()`` takes
+the datasets of a k-Wave HDF5 input file as a dict (the names written by
+``k-Wave/private/kspaceFirstOrder_saveToDisk.m``) and returns the datasets
+of the output file (the names read by ``k-Wave/kspaceFirstOrder3DC.m:569-776``).
+
+There is no fallback: if the shared library is missing, importing this
+module raises, and every solve runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("KWAVE_B200_LIB", os.path.join(os.path.dirname(_HERE), "libkwave_b200.so"))
+
+KW_OK = 0
+STATUS_NAMES = {0: "KW_OK", 1: "KW_ERR_INVALID_ARGUMENT", 2: "KW_ERR_CUDA", 3: "KW_ERR_OUT_OF_MEMORY",
+                4: "KW_ERR_IO", 5: "KW_ERR_UNSUPPORTED", 6: "KW_ERR_INTERNAL"}
+
+c_float_p = C.POINTER(C.c_float)
+c_u64_p = C.POINTER(C.c_uint64)
+
+
+class KwStatus(C.Structure):
+    _fields_ = [("code", C.c_int), ("message", C.c_char * 512)]
+
+
+class KwField(C.Structure):
+    _fields_ = [("data", c_float_p), ("numel", C.c_uint64)]
+
+
+class KwInput(C.Structure):
+    _fields_ = [
+        ("Nx", C.c_uint64), ("Ny", C.c_uint64), ("Nz", C.c_uint64), ("Nt", C.c_uint64),
+        ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float), ("dt", C.c_float),
+        ("c_ref", C.c_float),
+        ("pml_x_size", C.c_uint64), ("pml_y_size", C.c_uint64), ("pml_z_size", C.c_uint64),
+        ("pml_x_alpha", C.c_float), ("pml_y_alpha", C.c_float), ("pml_z_alpha", C.c_float),
+        ("c0", KwField), ("rho0", KwField),
+        ("rho0_sgx", KwField), ("rho0_sgy", KwField), ("rho0_sgz", KwField),
+        ("nonlinear_flag", C.c_uint64), ("BonA", KwField),
+        ("absorbing_flag", C.c_uint64), ("alpha_coeff", KwField), ("alpha_power", C.c_float),
+        ("p0_source_flag", C.c_uint64), ("p0_source_input", c_float_p),
+        ("p_source_flag", C.c_uint64), ("p_source_mode", C.c_uint64), ("p_source_many", C.c_uint64),
+        ("p_source_index", c_u64_p), ("p_source_index_numel", C.c_uint64),
+        ("p_source_input", c_float_p),
+        ("ux_source_flag", C.c_uint64), ("uy_source_flag", C.c_uint64), ("uz_source_flag", C.c_uint64),
+        ("u_source_mode", C.c_uint64), ("u_source_many", C.c_uint64),
+        ("u_source_index", c_u64_p), ("u_source_index_numel", C.c_uint64),
+        ("ux_source_input", c_float_p), ("uy_source_input", c_float_p), ("uz_source_input", c_float_p),
+        ("sensor_mask_type", C.c_uint64),
+        ("sensor_mask_index", c_u64_p), ("sensor_mask_index_numel", C.c_uint64),
+        ("sensor_mask_corners", c_u64_p), ("sensor_mask_corners_numel", C.c_uint64),
+    ]
+
+
+class KwOptions(C.Structure):
+    _fields_ = [
+        ("p_raw", C.c_int), ("p_max", C.c_int), ("p_min", C.c_int), ("p_rms", C.c_int),
+        ("p_max_all", C.c_int), ("p_min_all", C.c_int), ("p_final", C.c_int),
+        ("u_raw", C.c_int), ("u_max", C.c_int), ("u_min", C.c_int), ("u_rms", C.c_int),
+        ("u_max_all", C.c_int), ("u_min_all", C.c_int), ("u_final", C.c_int),
+        ("u_non_staggered_raw", C.c_int),
+        ("start_index", C.c_uint64), ("device", C.c_int), ("verbose", C.c_int),
+    ]
+
+
+OUTPUT_FIELDS = [
+    "p", "p_max", "p_min", "p_rms", "p_max_all", "p_min_all", "p_final",
+    "ux", "uy", "uz", "ux_max", "uy_max", "uz_max", "ux_min", "uy_min", "uz_min",
+    "ux_rms", "uy_rms", "uz_rms", "ux_max_all", "uy_max_all", "uz_max_all",
+    "ux_min_all", "uy_min_all", "uz_min_all", "ux_final", "uy_final", "uz_final",
+    "ux_non_staggered", "uy_non_staggered", "uz_non_staggered",
+]
+
+
+class KwOutput(C.Structure):
+    _fields_ = [(n, c_float_p) for n in OUTPUT_FIELDS]
+
+
+class KwOutputSizes(C.Structure):
+    _fields_ = [("num_sensor_points", C.c_uint64), ("num_recorded_steps", C.c_uint64),
+                ("grid_points", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
+EXPORTED = [
+    "kw_version", "kw_output_sizes_query", "kw_solve", "kw_run_file", "kw_cli_main",
+    "kw_session_create", "kw_session_advance", "kw_session_elapsed_ms", "kw_session_sync",
+    "kw_session_steps_done", "kw_session_read", "kw_session_stream", "kw_session_launches_per_step",
+    "kw_session_destroy",
+]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"kwave_b200 shared library not found at {LIB_PATH}; "
+                          "build it with `python k-wave_b200/build.py`")
+    lib = C.CDLL(LIB_PATH)
+    lib.kw_version.restype = C.c_char_p
+    lib.kw_output_sizes_query.argtypes = [C.POINTER(KwInput), C.POINTER(KwOptions),
+                                          C.POINTER(KwOutputSizes), C.POINTER(KwStatus)]
+    lib.kw_solve.argtypes = [C.POINTER(KwInput), C.POINTER(KwOptions), C.POINTER(KwOutput),
+                             C.POINTER(KwStatus)]
+    lib.kw_run_file.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(KwOptions), C.POINTER(KwStatus)]
+    lib.kw_cli_main.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
+    lib.kw_session_create.argtypes = [C.POINTER(KwInput), C.POINTER(KwOptions), C.POINTER(C.c_void_p),
+                                      C.POINTER(KwStatus)]
+    lib.kw_session_advance.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(KwStatus)]
+    lib.kw_session_elapsed_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(KwStatus)]
+    lib.kw_session_sync.argtypes = [C.c_void_p, C.POINTER(KwStatus)]
+    lib.kw_session_steps_done.argtypes = [C.c_void_p]
+    lib.kw_session_steps_done.restype = C.c_uint64
+    lib.kw_session_read.argtypes = [C.c_void_p, C.POINTER(KwOutput), C.POINTER(KwStatus)]
+    lib.kw_session_stream.argtypes = [C.c_void_p]
+    lib.kw_session_stream.restype = C.c_void_p
+    lib.kw_session_launches_per_step.argtypes = [C.c_void_p]
+    lib.kw_session_launches_per_step.restype = C.c_uint64
+    lib.kw_session_destroy.argtypes = [C.c_void_p]
+    return lib
+
+
+lib = _load()
+
+
+class KwaveError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def _check(code, st):
+    if code != KW_OK:
+        raise KwaveError(code, st.message.decode(errors="replace"))
+
+
+# ---------------------------------------------------------------------------
+# dict <-> struct
+# ---------------------------------------------------------------------------
+RECORD_TO_FLAG = {
+    "p": "p_raw", "p_max": "p_max", "p_min": "p_min", "p_rms": "p_rms", "p_max_all": "p_max_all",
+    "p_min_all": "p_min_all", "p_final": "p_final", "u": "u_raw", "u_max": "u_max", "u_min": "u_min",
+    "u_rms": "u_rms", "u_max_all": "u_max_all", "u_min_all": "u_min_all", "u_final": "u_final",
+    "u_non_staggered": "u_non_staggered_raw",
+}
+
+
+def make_options(record=("p",), start_index=1, device=-1, verbose=0):
+    o = KwOptions()
+    for r in record:
+        setattr(o, RECORD_TO_FLAG[r], 1)
+    o.start_index = int(start_index)
+    o.device = int(device)
+    o.verbose = int(verbose)
+    return o
+
+
+class _Keep:
+    """Holds the numpy arrays a KwInput points into."""
+
+    def __init__(self):
+        self.arrays = []
+
+    def f32(self, v):
+        a = np.ascontiguousarray(np.asarray(v, dtype=np.float32).reshape(-1, order="F"))
+        self.arrays.append(a)
+        return a
+
+    def u64(self, v):
+        a = np.ascontiguousarray(np.asarray(v, dtype=np.uint64).reshape(-1, order="F"))
+        self.arrays.append(a)
+        return a
+
+
+def _fptr(a):
+    return a.ctypes.data_as(c_float_p)
+
+
+def _uptr(a):
+    return a.ctypes.data_as(c_u64_p)
+
+
+def make_input(inp: dict):
+    """Build a KwInput from HDF5-file-level datasets.
+
+    Grid arrays are accepted in MATLAB axis order (shape (Nx, Ny[, Nz])) and
+    flattened x-fastest; signal matrices are (rows, Nt_src) as in MATLAB."""
+    keep = _Keep()
+    s = KwInput()
+    for k in ("Nx", "Ny", "Nz", "Nt"):
+        setattr(s, k, int(inp[k]))
+    for k in ("dx", "dy", "dz", "dt", "c_ref"):
+        setattr(s, k, float(inp.get(k, 0.0)))
+    for a in "xyz":
+        setattr(s, f"pml_{a}_size", int(inp.get(f"pml_{a}_size", 0)))
+        setattr(s, f"pml_{a}_alpha", float(inp.get(f"pml_{a}_alpha", 0.0)))
+
+    def fld(name):
+        if name not in inp or inp[name] is None:
+            return KwField()
+        a = keep.f32(inp[name])
+        return KwField(_fptr(a), a.size)
+
+    for name in ("c0", "rho0", "rho0_sgx", "rho0_sgy", "rho0_sgz", "BonA", "alpha_coeff"):
+        setattr(s, name, fld(name))
+    s.nonlinear_flag = int(inp.get("nonlinear_flag", 0))
+    s.absorbing_flag = int(inp.get("absorbing_flag", 0))
+    s.alpha_power = float(inp.get("alpha_power", 0.0))
+    s.p0_source_flag = int(inp.get("p0_source_flag", 0))
+    if s.p0_source_flag:
+        s.p0_source_input = _fptr(keep.f32(inp["p0_source_input"]))
+    s.p_source_flag = int(inp.get("p_source_flag", 0))
+    if s.p_source_flag:
+        s.p_source_mode = int(inp["p_source_mode"])
+        s.p_source_many = int(inp.get("p_source_many", 0))
+        idx = keep.u64(inp["p_source_index"])
+        s.p_source_index = _uptr(idx)
+        s.p_source_index_numel = idx.size
+        sig = np.asarray(inp["p_source_input"], dtype=np.float32)
+        sig = sig.reshape(-1, sig.shape[-1]) if sig.ndim > 1 else sig.reshape(1, -1)
+        # [rows, t] column-major == [t][rows] row-fastest
+        s.p_source_input = _fptr(keep.f32(sig))
+    u_any = False
+    for a in "xyz":
+        fl = int(inp.get(f"u{a}_source_flag", 0))
+        setattr(s, f"u{a}_source_flag", fl)
+        if fl:
+            u_any = True
+            sig = np.asarray(inp[f"u{a}_source_input"], dtype=np.float32)
+            sig = sig.reshape(-1, sig.shape[-1]) if sig.ndim > 1 else sig.reshape(1, -1)
+            setattr(s, f"u{a}_source_input", _fptr(keep.f32(sig)))
+    if u_any:
+        s.u_source_mode = int(inp["u_source_mode"])
+        s.u_source_many = int(inp.get("u_source_many", 0))
+        idx = keep.u64(inp["u_source_index"])
+        s.u_source_index = _uptr(idx)
+        s.u_source_index_numel = idx.size
+    s.sensor_mask_type = int(inp.get("sensor_mask_type", 0))
+    if s.sensor_mask_type == 0:
+        idx = keep.u64(inp["sensor_mask_index"])
+        s.sensor_mask_index = _uptr(idx)
+        s.sensor_mask_index_numel = idx.size
+    else:
+        cor = keep.u64(np.asarray(inp["sensor_mask_corners"]).reshape(6, -1))
+        s.sensor_mask_corners = _uptr(cor)
+        s.sensor_mask_corners_numel = cor.size
+    return s, keep
+
+
+def output_sizes(inp_struct, opt):
+    st = KwStatus()
+    sz = KwOutputSizes()
+    _check(lib.kw_output_sizes_query(C.byref(inp_struct), C.byref(opt), C.byref(sz), C.byref(st)), st)
+    return sz
+
+
+def alloc_outputs(inp: dict, record, sizes):
+    """Host buffers (numpy) for the requested outputs and the KwOutput struct."""
+    dim = 2 if int(inp["Nz"]) == 1 else 3
+    ns, nr, ng = sizes.num_sensor_points, sizes.num_recorded_steps, sizes.grid_points
+    comps = "xyz"[:dim]
+    bufs = {}
+    rec = set(record)
+    if "p" in rec:
+        bufs["p"] = np.zeros((nr, ns), np.float32)
+    for k in ("p_max", "p_min", "p_rms"):
+        if k in rec:
+            bufs[k] = np.zeros(ns, np.float32)
+    for k in ("p_max_all", "p_min_all", "p_final"):
+        if k in rec:
+            bufs[k] = np.zeros(ng, np.float32)
+    for c in comps:
+        if "u" in rec:
+            bufs["u" + c] = np.zeros((nr, ns), np.float32)
+        for k in ("max", "min", "rms"):
+            if "u_" + k in rec:
+                bufs[f"u{c}_{k}"] = np.zeros(ns, np.float32)
+        for k in ("max_all", "min_all", "final"):
+            if "u_" + k in rec:
+                bufs[f"u{c}_{k}"] = np.zeros(ng, np.float32)
+        if "u_non_staggered" in rec:
+            bufs[f"u{c}_non_staggered"] = np.zeros((nr, ns), np.float32)
+    out = KwOutput()
+    for k, v in bufs.items():
+        setattr(out, k, _fptr(v))
+    return out, bufs
+
+
+def to_matlab_layout(bufs: dict, inp: dict):
+    """Convert output buffers to the reference's array shapes: time series
+    (Ns, Nt_rec); per-point (Ns,); grid outputs (Nx, Ny[, Nz])."""
+    dim = 2 if int(inp["Nz"]) == 1 else 3
+    shape = (int(inp["Nx"]), int(inp["Ny"])) + ((int(inp["Nz"]),) if dim == 3 else ())
+    res = {}
+    for k, v in bufs.items():
+        if v.ndim == 2:
+            res[k] = v.T
+        elif k.endswith("_all") or k.endswith("_final"):
+            res[k] = v.reshape(shape, order="F")
+        else:
+            res[k] = v
+    return res
+
+
+def solve(inp: dict, record=("p",), start_index=1, device=-1):
+    """kw_solve(): one simulation, host buffers in and out."""
+    s, keep = make_input(inp)
+    opt = make_options(record, start_index, device)
+    sizes = output_sizes(s, opt)
+    out, bufs = alloc_outputs(inp, record, sizes)
+    st = KwStatus()
+    _check(lib.kw_solve(C.byref(s), C.byref(opt), C.byref(out), C.byref(st)), st)
+    del keep
+    return to_matlab_layout(bufs, inp)
+
+
+class Session:
+    """A resident simulation advanced in steps (kw_session_*)."""
+
+    def __init__(self, inp: dict, record=("p",), start_index=1, device=-1):
+        self.inp = inp
+        self.record = tuple(record)
+        self._s, self._keep = make_input(inp)
+        self._opt = make_options(record, start_index, device)
+        self.sizes = output_sizes(self._s, self._opt)
+        h = C.c_void_p()
+        st = KwStatus()
+        _check(lib.kw_session_create(C.byref(self._s), C.byref(self._opt), C.byref(h), C.byref(st)), st)
+        self._h = h
+
+    def advance(self, n):
+        st = KwStatus()
+        _check(lib.kw_session_advance(self._h, C.c_uint64(int(n)), C.byref(st)), st)
+
+    def elapsed_ms(self):
+        st = KwStatus()
+        ms = C.c_float()
+        _check(lib.kw_session_elapsed_ms(self._h, C.byref(ms), C.byref(st)), st)
+        return ms.value
+
+    def sync(self):
+        st = KwStatus()
+        _check(lib.kw_session_sync(self._h, C.byref(st)), st)
+
+    @property
+    def steps_done(self):
+        return int(lib.kw_session_steps_done(self._h))
+
+    @property
+    def stream(self):
+        return lib.kw_session_stream(self._h)
+
+    @property
+    def launches_per_step(self):
+        return int(lib.kw_session_launches_per_step(self._h))
+
+    def read(self):
+        out, bufs = alloc_outputs(self.inp, self.record, self.sizes)
+        st = KwStatus()
+        _check(lib.kw_session_read(self._h, C.byref(out), C.byref(st)), st)
+        return to_matlab_layout(bufs, self.inp)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.kw_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def version():
+    return lib.kw_version().decode()

@@ -1,0 +1,148 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on
+the same seeded inputs.
+
+Tolerances (relative L2 over each output array): 1e-5 for linear lossless
+runs and 1e-4 otherwise, against the FP64 oracle (the reference with
+DataCast 'off'); the FP32 oracle is checked at the same bars.
+"""
+import numpy as np
+import pytest
+
+from helpers import case_2d_p0, case_3d_het, compare, oracle_outputs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_LOSSLESS = 1e-5
+TOL = 1e-4
+
+
+def _solve(inp, record, start=1):
+    from kwave import _lib
+
+    return _lib.solve(inp, record=record, start_index=start)
+
+
+def _check(inp, record, tol, start=1):
+    gpu = _solve(inp, record, start)
+    for dt in (np.float64, np.float32):
+        ora = oracle_outputs(inp, record, start, dtype=dt)
+        errs = compare(gpu, ora)
+        assert errs, "no common outputs"
+        bad = {k: v for k, v in errs.items() if not v <= tol}
+        assert not bad, f"{np.dtype(dt).name} oracle: {bad}"
+    return gpu
+
+
+def test_2d_p0_lossless_all_records():
+    inp, record, start, _ = case_2d_p0()
+    _check(inp, record, TOL_LOSSLESS)
+
+
+def test_2d_p0_odd_sizes():
+    inp, record, start, _ = case_2d_p0(n=(45, 50), nt=60, record=("p", "p_max", "u", "p_final"))
+    _check(inp, record, TOL_LOSSLESS)
+
+
+def test_3d_p0_lossless():
+    from kwave.simulation import prepare
+    from kwave.utils import KWaveGrid, make_ball
+
+    n = (32, 30, 27)
+    kg = KWaveGrid(n, (1e-4, 1e-4, 1e-4))
+    kg.set_time(50, 0.3e-4 / 1500)
+    p0 = make_ball(*n, 16, 15, 14, 4)
+    mask = np.zeros(n)
+    mask[4:28:5, 3:27:4, 2:25:6] = 1
+    inp, record, start, _ = prepare(kg, {"sound_speed": 1500.0, "density": 1000.0}, {"p0": p0},
+                                    {"mask": mask, "record": ["p", "u", "p_max", "p_rms", "p_final",
+                                                              "u_final", "p_min_all"]}, pml_size=5)
+    _check(inp, record, TOL_LOSSLESS)
+
+
+def test_3d_heterogeneous_absorbing_nonlinear_additive_source():
+    inp, record, start, _ = case_3d_het()
+    _check(inp, record, TOL)
+
+
+def test_3d_stokes_dirichlet_source():
+    inp, record, start, _ = case_3d_het(stokes=True, p_mode="dirichlet", nonlinear=False)
+    _check(inp, record, TOL)
+
+
+def test_3d_additive_no_correction_many_signals():
+    inp, record, start, _ = case_3d_het(p_mode="additive-no-correction", many=True, absorbing=False)
+    _check(inp, record, TOL)
+
+
+def test_3d_additive_many_signals():
+    inp, record, start, _ = case_3d_het(p_mode="additive", many=True, nonlinear=False)
+    _check(inp, record, TOL)
+
+
+def test_record_start_index():
+    inp, record, start, _ = case_2d_p0(record=("p", "p_max", "p_rms", "u_rms"))
+    _check(inp, record, TOL_LOSSLESS, start=17)
+
+
+@pytest.mark.parametrize("mode", ["dirichlet", "additive", "additive-no-correction"])
+def test_2d_velocity_sources(mode):
+    from kwave.simulation import prepare
+    from kwave.utils import KWaveGrid, tone_burst
+
+    n = (48, 40)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    kg.set_time(70, 0.3e-4 / 1500)
+    umask = np.zeros(n)
+    umask[10, 12:28] = 1
+    sig = tone_burst(1 / kg.dt, 3e6, 2)
+    source = {"u_mask": umask, "ux": sig, "uy": 0.5 * sig, "u_mode": mode}
+    smask = np.zeros(n)
+    smask[20:40:3, 5:35:4] = 1
+    inp, record, start, _ = prepare(kg, {"sound_speed": 1500.0, "density": 1000.0}, source,
+                                    {"mask": smask, "record": ["p", "u", "u_max"]}, pml_size=6)
+    _check(inp, record, TOL_LOSSLESS)
+
+
+def test_cuboid_equals_binary_mask():
+    """kspaceFirstOrder3D_compare_binary_and_cuboid_sensor_mask.m: the same
+    points recorded through cuboid corners and through a binary mask."""
+    from kwave.simulation import prepare
+    from kwave.utils import KWaveGrid, make_ball
+
+    n = (30, 32, 36)
+    kg = KWaveGrid(n, (1e-4, 1e-4, 1e-4))
+    kg.set_time(40, 0.3e-4 / 1500)
+    p0 = make_ball(*n, 15, 16, 18, 3)
+    corners = np.array([[4, 5, 6, 10, 12, 9], [20, 18, 25, 24, 22, 30]]).T
+    rec = ["p", "p_max", "u"]
+    inp_c, record, _, meta = prepare(kg, {"sound_speed": 1500.0, "density": 1000.0}, {"p0": p0},
+                                     {"mask": corners, "record": rec}, pml_size=5)
+    mask = np.zeros(n)
+    lin = []
+    for k in range(corners.shape[1]):
+        x1, y1, z1, x2, y2, z2 = corners[:, k]
+        sub = np.zeros(n, dtype=bool)
+        sub[x1 - 1:x2, y1 - 1:y2, z1 - 1:z2] = True
+        lin.append(np.flatnonzero(sub.reshape(-1, order="F")) + 1)
+    inp_b = dict(inp_c)
+    inp_b.pop("sensor_mask_corners")
+    inp_b["sensor_mask_type"] = 0
+    inp_b["sensor_mask_index"] = np.concatenate(lin)
+    a = _solve(inp_c, record)
+    b = _solve(inp_b, record)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_output_sizes_and_errors():
+    from kwave import _lib
+
+    inp, record, start, _ = case_2d_p0()
+    bad = dict(inp)
+    bad["sensor_mask_index"] = np.array([0, 5])
+    with pytest.raises(_lib.KwaveError):
+        _solve(bad, record)
+    bad = dict(inp)
+    bad["Nx"] = 7 * 8
+    with pytest.raises(_lib.KwaveError):
+        _solve(bad, record)
