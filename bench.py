@@ -1,0 +1,317 @@
+"""Benchmark: grid-point-steps/s of the k-space fluid time loop.
+
+Workload: 3D 256^3 (PML 10 inside), heterogeneous (smoothed-noise c and rho),
+power-law absorbing (alpha 0.75 dB/(MHz^y cm), y 1.5), nonlinear (B/A 6),
+48x48 additive plane pressure source (1 MHz 3-cycle tone burst, 1 MPa),
+every grid point a sensor recording p_max and p_rms, Nt 1200, FP32.
+
+A "step" is one time step of that simulation.  `value` is measured with the
+simulation resident in HBM (kw_session_advance, CUDA events on the session's
+stream); `e2e` is a whole solve through the C ABI (kw_solve) from pinned
+host buffers, host<->device copies included.  Every field (1.1 GB working
+set) is larger than the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: each rank runs its own independent simulation ("replicas
+only": one simulation does not shard), so `value` sums over ranks.
+
+`--impl reference` times the reference algorithm on the host CPU instead:
+the reference's own implementation is MATLAB (not installable here), so the
+CPU restatement in oracle/ (numpy + scipy.fft on all host threads) stands
+in for it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "k-wave_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt-steps/s at 256^3 FP32 (heterogeneous absorbing nonlinear)"
+UNIT = "grid-pt-steps/s"
+B_ALG = 232.0  # algorithmic bytes per grid-point-step (58 FP32 full-grid arrays)
+WORKLOAD = "3D 256^3 het absorbing nonlinear, additive plane p source, all-point p_max/p_rms, Nt 1200, FP32"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_input(n, nt):
+    from kwave.simulation import prepare
+    from kwave.workloads import het_absorbing_3d
+
+    kg, medium, source, sensor = het_absorbing_3d(n=n, nt=nt)
+    inp, record, start, _ = prepare(kg, medium, source, sensor)
+    return inp, record, start
+
+
+def pin_inputs(inp):
+    """Copy every array input into pinned host memory, flattened x-fastest."""
+    import torch
+
+    out = {}
+    npts = int(inp["Nx"]) * int(inp["Ny"]) * int(inp["Nz"])
+    for k, v in inp.items():
+        if isinstance(v, np.ndarray) and (v.size == npts or k.endswith("index")):
+            dt = np.uint64 if k.endswith("index") or k.endswith("corners") else np.float32
+            flat = np.asarray(v).reshape(-1, order="F").astype(dt)
+            t = torch.empty(flat.size, dtype=torch.float32 if dt == np.float32 else torch.int64, pin_memory=True)
+            a = t.numpy()
+            if dt == np.uint64:
+                a = a.view(np.uint64)
+            a[...] = flat
+            out[k] = a
+            out["_pin_" + k] = t
+        else:
+            out[k] = v
+    return out
+
+
+def h2d_bytes(inp):
+    b = 0
+    for k, v in inp.items():
+        if k.startswith("_pin_"):
+            continue
+        if isinstance(v, np.ndarray):
+            b += v.nbytes if v.dtype != np.float64 else v.size * 4
+    return b
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_per_step(n):
+    """DRAM bytes per step from the committed ncu summary (scaled to n^3)."""
+    path = os.path.join(ROOT, "profiles", "step_het_absorbing_traffic.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_grid_point_step:\s*([0-9.eE+-]+)", txt)
+    if not m:
+        return None
+    return float(m.group(1)) * n ** 3
+
+
+def cpu_sample(inp, record, steps=3, warmup=2):
+    """Time the oracle (numpy/scipy, all host threads) on the first
+    warmup+steps time steps of the same workload."""
+    from oracle.kspace_oracle import simulate
+
+    stamps = []
+    simulate(inp, record=record, dtype=np.float32, workers=-1, max_steps=warmup + steps,
+             on_step=lambda t: stamps.append(time.perf_counter()))
+    per = (stamps[-1] - stamps[warmup - 1]) / steps
+    npts = int(inp["Nx"]) * int(inp["Ny"]) * int(inp["Nz"])
+    return npts / per, per
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    inp, record, start = build_input(args.n, args.nt)
+    from oracle.kspace_oracle import simulate
+
+    npts = args.n ** 3
+    # bounded sample: warm-up steps plus timed steps, capped at ~3 minutes
+    stamps = []
+    w = max(1, min(args.warmup, 3))
+    t0 = time.perf_counter()
+    probe = []
+    simulate(inp, record=record, dtype=np.float32, workers=-1, max_steps=w + 1,
+             on_step=lambda t: probe.append(time.perf_counter()))
+    per_est = probe[-1] - probe[-2]
+    k = max(1, min(args.steps, int(150.0 / max(per_est, 1e-3))))
+    simulate(inp, record=record, dtype=np.float32, workers=-1, max_steps=w + k,
+             on_step=lambda t: stamps.append(time.perf_counter()))
+    per = (stamps[-1] - stamps[w - 1]) / k
+    value = npts / per
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": k, "warmup": w, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "Nt": args.nt},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"time steps {w + 1}..{w + k} of the {args.n}^3 run, numpy/scipy.fft "
+                                   f"workers={cores}; MATLAB reference not installable here"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--nt", type=int, default=1200)
+    ap.add_argument("--e2e-reps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    from kwave import _lib
+
+    inp, record, start = build_input(args.n, args.nt)
+    nt_needed = args.warmup + args.steps
+    sess_inp = dict(inp)
+    if nt_needed > int(inp["Nt"]):
+        sess_inp["Nt"] = nt_needed
+    pinned = pin_inputs(sess_inp)
+    npts = args.n ** 3
+
+    # ----- device-resident timing -----
+    sess = _lib.Session(pinned, record=record, start_index=start, device=local)
+    sess.advance(args.warmup)
+    sess.sync()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    sess.advance(args.steps)
+    ms = sess.elapsed_ms()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches_per_step = sess.launches_per_step
+    sess.close()
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * npts * args.steps / (ms_max / 1e3)
+    ms_per_step = ms_max / args.steps
+
+    # ----- end to end: a whole solve through kw_solve from pinned host memory -----
+    e2e_inp = pin_inputs(inp)
+    e2e_vals = []
+    d2h = npts * 4 * sum(1 for r in record if r in ("p_max", "p_rms", "p_min"))
+    for _ in range(args.e2e_reps):
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.solve(e2e_inp, record=record, start_index=start, device=local)
+        torch.cuda.synchronize()
+        dt_e2e = time.perf_counter() - t0
+        t_t = torch.tensor([dt_e2e], device="cuda")
+        if dist is not None:
+            dist.all_reduce(t_t, op=dist.ReduceOp.MAX)
+        e2e_vals.append(world * npts * int(inp["Nt"]) / float(t_t.item()))
+    e2e_value = max(e2e_vals) if e2e_vals else None
+
+    peak, peak_kind = peaks()
+    achieved = B_ALG * npts / (ms_per_step / 1e3) / 1e9
+    traffic = traffic_per_step(args.n)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "Nt": int(inp["Nt"]),
+                   "parallelism": f"replicas{world}", "l2": "working set 1.1 GB > 126 MB L2, no flush needed"},
+        "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes(inp), "d2h_bytes_per_step": d2h,
+                 "note": f"one e2e step = one whole {int(inp['Nt'])}-step solve via kw_solve, pinned host buffers"}
+                if e2e_value else None),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "unit_of_work": f"one time step ({B_ALG:.0f} B algorithmic per grid point)"},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, per = cpu_sample(inp, record)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"time steps 3..5 of the same {args.n}^3 run, oracle (numpy/scipy.fft, "
+                                          f"all host threads), {per:.2f} s/step"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

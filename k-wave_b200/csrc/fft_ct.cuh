@@ -1,0 +1,145 @@
+// Compile-time-sized line FFTs (the fast path of the solver's FFT engine).
+//
+// For a transform length N known at compile time, the radix plan, the
+// per-stage butterfly counts, the thread -> butterfly mapping and every
+// index division fold to constants.  T = N / RMAX threads cooperate on one
+// line; in stage s each thread runs ceil((N / R_s) / T) radix-R_s butterflies
+// held in registers.  Stages run in place: all butterfly inputs of a thread
+// are loaded to registers, the block synchronises, and the outputs are
+// written back to the same buffer, so a transform needs a single shared-
+// memory tile (one buffer per field instead of a ping-pong pair).
+#pragma once
+#include "fft_engine.cuh"
+
+namespace kwb {
+
+// The compile-time plan, chosen so the largest radix sets T = N / RMAX
+// threads per line: 16-point stages first, then 8 / 4 / 2, then 5, 3.
+__host__ __device__ constexpr int ct_stage_count(int n) {
+  if (n <= 0) return -1;
+  int m = n, s = 0;
+  while (m % 16 == 0) { m /= 16; ++s; }
+  const int rs[5] = {8, 4, 2, 5, 3};
+  for (int i = 0; i < 5; ++i)
+    while (m % rs[i] == 0) { m /= rs[i]; ++s; }
+  return m == 1 ? s : -1;
+}
+
+__host__ __device__ constexpr int ct_radix(int n, int stage) {
+  if (n <= 0) return 1;
+  int m = n, s = 0;
+  while (m % 16 == 0) {
+    if (s == stage) return 16;
+    m /= 16;
+    ++s;
+  }
+  const int rs[5] = {8, 4, 2, 5, 3};
+  for (int i = 0; i < 5; ++i)
+    while (m % rs[i] == 0) {
+      if (s == stage) return rs[i];
+      m /= rs[i];
+      ++s;
+    }
+  return 1;
+}
+
+__host__ __device__ constexpr int ct_ns(int n, int stage) {  // product of the radices before `stage`
+  int p = 1;
+  for (int s = 0; s < stage; ++s) p *= ct_radix(n, s);
+  return p;
+}
+
+__host__ __device__ constexpr int ct_rmax(int n) {
+  int r = 1;
+  for (int s = 0; s < ct_stage_count(n); ++s) r = ct_radix(n, s) > r ? ct_radix(n, s) : r;
+  return r;
+}
+
+template <int N>
+struct Ct {
+  static constexpr int S = ct_stage_count(N);
+  static constexpr int RMAX = ct_rmax(N);
+  static constexpr int T = N / RMAX;  // threads per line
+  static_assert(S > 0, "transform length must factor into 2, 3 and 5");
+};
+
+// Lines per thread block for a compile-time length: about 256 threads, at
+// least 4 lines (a 32-byte sector of complex values per column tile row).
+__host__ __device__ constexpr int ct_lines_of(int n) {
+  if (n <= 0) return 0;
+  int l = 256 / (n / ct_rmax(n));
+  if (l < 4) l = 4;
+  if (l > 32) l = 32;
+  return l;
+}
+__host__ __device__ constexpr int ct_threads_of(int n) { return n <= 0 ? 0 : (n / ct_rmax(n)) * ct_lines_of(n); }
+
+template <int N, int STAGE, bool INV, class L>
+__device__ __forceinline__ void ct_stage(float2* buf, const float2* __restrict__ tw, int l, int tid, L lay) {
+  constexpr int R = ct_radix(N, STAGE);
+  constexpr int NS = ct_ns(N, STAGE);
+  constexpr int NR = N / R;
+  constexpr int T = Ct<N>::T;
+  constexpr int NB = (NR + T - 1) / T;
+  constexpr int TWS = N / (NS * R);
+  float2 v[NB][R];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = tid + i * T;
+    if (NR % T == 0 || j < NR) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = buf[lay(l, j + r * NR)];
+      if constexpr (NS > 1) {
+        const int k = j % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = tw[k * r * TWS];
+          if (INV) w.y = -w.y;
+          v[i][r] = c_mul(v[i][r], w);
+        }
+      }
+      dft<R, INV>(v[i]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = tid + i * T;
+    if (NR % T == 0 || j < NR) {
+      const int k = j % NS;
+      const int idx = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[lay(l, idx + r * NS)] = v[i][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int STAGE, bool INV, class L>
+__device__ __forceinline__ void ct_stages(float2* buf, const float2* __restrict__ tw, int l, int tid, L lay) {
+  if constexpr (STAGE < Ct<N>::S) {
+    ct_stage<N, STAGE, INV>(buf, tw, l, tid, lay);
+    ct_stages<N, STAGE + 1, INV>(buf, tw, l, tid, lay);
+  }
+}
+
+// In-place transform of LINES lines by T * LINES threads.  LINE_FAST maps
+// consecutive threads to consecutive lines (column tiles, whose lines are
+// adjacent in shared memory); otherwise to consecutive butterflies of one
+// line (row tiles).  Must be called by every thread of the block (it
+// synchronises); the caller synchronises before the call.
+template <int N, bool INV, bool LINE_FAST, int LINES, class L>
+__device__ __forceinline__ void ct_fft(float2* buf, const float2* __restrict__ tw, L lay) {
+  constexpr int T = Ct<N>::T;
+  int l, tid;
+  if (LINE_FAST) {
+    l = threadIdx.x % LINES;
+    tid = threadIdx.x / LINES;
+  } else {
+    l = threadIdx.x / T;
+    tid = threadIdx.x - l * T;
+  }
+  ct_stages<N, 0, INV>(buf, tw, l, tid, lay);
+}
+
+}  // namespace kwb

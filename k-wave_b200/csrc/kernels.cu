@@ -12,72 +12,63 @@
 // R2C so each field row is read and written once.  The y axis (3D) is a
 // column pass (k_col_fft) and the last axis (z in 3D, y in 2D) is done by
 // k_fused_last: forward, operator multiply, inverse, in one kernel.
+//
+// Every FFT-carrying kernel is a template on NC, the length of the axis it
+// transforms: NC > 0 selects the compile-time engine (fft_ct.cuh: in-place
+// register-staged stages, one shared-memory buffer per field, index math
+// folded to constants); NC == 0 is the runtime-plan engine for any other
+// 2^a 3^b 5^c length.
+#include "fft_ct.cuh"
 #include "kernels.cuh"
+#include "spec_ops.cuh"
 
 namespace kwb {
 
-// ---------------------------------------------------------------------------
-// spectral operators generated per point from 1D tables
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 eval_op(const SpecOp& op, const SpecTables& T, int dim, int ix,
-                                          int iy, int iz) {
-  float k2 = __ldg(T.k2[0] + ix) + __ldg(T.k2[1] + iy);
-  if (dim == 3) k2 += __ldg(T.k2[2] + iz);
-  const float k = sqrtf(k2);
-  switch (op.kind) {
-    case OP_GRAD_POS:
-    case OP_GRAD_NEG: {
-      // kappa = sinc(c_ref k dt / 2), sinc(x) = sin(x) / x (k-Wave/private/sinc.m:38-39)
-      const float x = T.cdt2 * k;
-      const float kap = (x == 0.f) ? 1.f : sinf(x) / x;
-      const int id = op.axis == 0 ? ix : (op.axis == 1 ? iy : iz);
-      const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
-      const float2 d = tab[id];
-      const float s = kap * T.scale;
-      return make_float2(d.x * s, d.y * s);
-    }
-    case OP_NABLA1:
-    case OP_NABLA2: {
-      // k.^(y-2) / k.^(y-1) with the infinite value at k = 0 set to zero
-      // (kspaceFirstOrder_createAbsorptionVariables.m:37-39, 49-51)
-      const float e = (op.kind == OP_NABLA1) ? T.ym2 : T.ym1;
-      float v;
-      if (k == 0.f)
-        v = (e == 0.f) ? 1.f : 0.f;
-      else
-        v = powf(k, e);
-      return make_float2(v * T.scale, 0.f);
-    }
-    case OP_SRC_KAPPA: {
-      const float x = T.cdt2 * k;
-      return make_float2(cosf(x) * T.scale, 0.f);
-    }
-    default:
-      return make_float2(T.scale, 0.f);
+// Lines per block / threads per block of a kernel instantiation.
+template <int NC>
+struct Tile {
+  static constexpr int LINES = ct_lines_of(NC);
+  static constexpr int THREADS = NC > 0 ? ct_threads_of(NC) : kThreads;
+};
+
+// Transform the lines of a tile.  Compile-time lengths run in place in `a`;
+// the runtime engine ping-pongs with `b`.  Returns the result buffer.
+template <int NC, bool INV, bool COL, class L>
+__device__ __forceinline__ float2* tile_fft(float2* a, float2* b, const float2* __restrict__ tw,
+                                            const FFTPlan& plan, int nlines, L lay) {
+  if constexpr (NC > 0) {
+    ct_fft<NC, INV, COL, Tile<NC>::LINES>(a, tw, lay);
+    return a;
+  } else {
+    return fft_lines<INV, COL>(a, b, tw, plan, nlines, lay);
   }
 }
 
 // ---------------------------------------------------------------------------
 // column passes
 // ---------------------------------------------------------------------------
-template <bool INV>
-__global__ void __launch_bounds__(kThreads) k_col_fft(ColArgs a, FFTPlan plan,
-                                                      const float2* __restrict__ tw_g) {
+template <int NC, bool INV>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_col_fft(ColArgs a, const __grid_constant__ FFTPlan plan,
+                                                               const float2* __restrict__ tw_g) {
   extern __shared__ float2 sm[];
-  const int n = plan.n, tl = a.tl;
+  constexpr bool CT = NC > 0;
+  const int n = CT ? NC : plan.n;
+  const int tl = CT ? Tile<NC>::LINES : a.tl;
   float2* tw = sm;
   float2* b0 = sm + n;
-  float2* b1 = b0 + tl * n;
+  float2* b1 = CT ? nullptr : b0 + tl * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
   float2* g = a.buf[blockIdx.z] + (long long)blockIdx.y * a.ostride;
   const int c0 = blockIdx.x * tl;
   const int total = tl * n;
+#pragma unroll 4
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int l = i % tl, p = i / tl, c = c0 + l;
     b0[i] = (c < a.ncols) ? g[p * a.lstride + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* r = fft_lines<INV, true>(b0, b1, tw, plan, tl, ColLayout{tl});
+  float2* r = tile_fft<NC, INV, true>(b0, b1, tw, plan, tl, ColLayout{tl});
+#pragma unroll 4
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int l = i % tl, p = i / tl, c = c0 + l;
     if (c < a.ncols) g[p * a.lstride + c] = r[i];
@@ -86,15 +77,19 @@ __global__ void __launch_bounds__(kThreads) k_col_fft(ColArgs a, FFTPlan plan,
 
 // Last axis: forward transform, multiply by `fanout` operators, inverse
 // transform each product.
-__global__ void __launch_bounds__(kThreads) k_fused_last(FusedArgs a, FFTPlan plan,
-                                                         const float2* __restrict__ tw_g,
-                                                         SpecTables T, int dim) {
+template <int NC>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_fused_last(const __grid_constant__ FusedArgs a,
+                                                                  const __grid_constant__ FFTPlan plan,
+                                                                  const float2* __restrict__ tw_g,
+                                                                  const __grid_constant__ SpecTables T, int dim) {
   extern __shared__ float2 sm[];
-  const int n = plan.n, tl = a.tl;
+  constexpr bool CT = NC > 0;
+  const int n = CT ? NC : plan.n;
+  const int tl = CT ? Tile<NC>::LINES : a.tl;
   float2* tw = sm;
   float2* A = sm + n;
   float2* B = A + tl * n;
-  float2* C = B + tl * n;
+  float2* C = CT ? nullptr : B + tl * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
   const int g = blockIdx.z;
   const int outer = blockIdx.y;
@@ -102,13 +97,14 @@ __global__ void __launch_bounds__(kThreads) k_fused_last(FusedArgs a, FFTPlan pl
   const float2* src = a.in[g] + off;
   const int c0 = blockIdx.x * tl;
   const int total = tl * n;
+#pragma unroll 4
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int l = i % tl, p = i / tl, c = c0 + l;
     A[i] = (c < a.ncols) ? src[p * a.lstride + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const ColLayout lay{tl};
-  float2* F = fft_lines<false, true>(A, B, tw, plan, tl, lay);
+  float2* F = tile_fft<NC, false, true>(A, B, tw, plan, tl, lay);
   float2* W1 = (F == A) ? B : A;
   float2* W2 = C;
   for (int o = 0; o < a.fanout; ++o) {
@@ -117,14 +113,14 @@ __global__ void __launch_bounds__(kThreads) k_fused_last(FusedArgs a, FFTPlan pl
       const int l = i % tl, p = i / tl;
       int c = c0 + l;
       if (c >= a.ncols) c = 0;
-      const int ix = c;
       const int iy = (dim == 3) ? outer : p;
       const int iz = (dim == 3) ? p : 0;
-      W1[i] = c_mul(F[i], eval_op(op, T, dim, ix, iy, iz));
+      W1[i] = c_mul(F[i], eval_op(op, T, dim, c, iy, iz));
     }
     __syncthreads();
-    float2* R = fft_lines<true, true>(W1, W2, tw, plan, tl, lay);
+    float2* R = tile_fft<NC, true, true>(W1, W2, tw, plan, tl, lay);
     float2* dst = a.out[g * a.fanout + o] + off;
+#pragma unroll 4
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int l = i % tl, p = i / tl, c = c0 + l;
       if (c < a.ncols) dst[p * a.lstride + c] = R[i];
@@ -149,10 +145,40 @@ __device__ __forceinline__ void set_comp(float2* b, RowLayout lay, int q, int x,
 // Build the full complex spectrum of each packed line from two half spectra
 // (C2R).  The imaginary parts of the k = 0 and Nyquist bins are dropped,
 // which is the Hermitian projection that real(ifftn(.)) performs.
-__device__ void load_c2r(const float2* __restrict__ S, float2* buf, RowLayout lay, const Dims& d,
-                         long long r0, int L) {
-  const int n = d.nx;
+template <int NC>
+__device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* buf, RowLayout lay, const Dims& d,
+                                         long long r0, int L) {
+  if constexpr (NC > 0 && NC % 4 == 0) {
+    // paired 16-byte loads; each loaded bin k also fills its mirror n - k
+    constexpr int n = NC, np = NC / 4 + 1;  // bin pairs (k, k+1), k even, k <= n/2
+    const int total = L * np;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int l = i / np, k = 2 * (i - l * np);
+      const long long ra = r0 + 2 * l, rb = ra + 1;
+      float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
+      if (ra < d.nrows) A = *reinterpret_cast<const float4*>(S + ra * d.nxp + k);
+      if (rb < d.nrows) B = *reinterpret_cast<const float4*>(S + rb * d.nxp + k);
+      if (k == 0) {
+        A.y = 0.f;
+        B.y = 0.f;
+      }
+      if (2 * k == n) {
+        A.y = 0.f;
+        B.y = 0.f;
+      }
+      buf[lay(l, k)] = make_float2(A.x - B.y, A.y + B.x);
+      if (k > 0 && 2 * k < n) buf[lay(l, n - k)] = make_float2(A.x + B.y, B.x - A.y);
+      if (2 * (k + 1) < n) {
+        buf[lay(l, k + 1)] = make_float2(A.z - B.w, A.w + B.z);
+        buf[lay(l, n - k - 1)] = make_float2(A.z + B.w, B.z - A.w);
+      }
+    }
+    return;
+  }
+  const int n = NC > 0 ? NC : d.nx;
   const int total = L * n;
+#pragma unroll 4
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int l = i / n, k = i - l * n;
     const long long ra = r0 + 2 * l, rb = ra + 1;
@@ -173,10 +199,36 @@ __device__ void load_c2r(const float2* __restrict__ S, float2* buf, RowLayout la
 
 // Split each packed line's spectrum Z = FFT(a + i b) into the half spectra
 // of a and b (R2C) and store them.
-__device__ void store_r2c(const float2* buf, float2* __restrict__ S, RowLayout lay, const Dims& d,
-                          long long r0, int L) {
-  const int n = d.nx, nh = d.nxh;
+template <int NC>
+__device__ __forceinline__ void store_r2c(const float2* buf, float2* __restrict__ S, RowLayout lay, const Dims& d,
+                                          long long r0, int L) {
+  if constexpr (NC > 0 && NC % 4 == 0) {
+    constexpr int n = NC, nh = NC / 2 + 1, np = NC / 4 + 1;
+    const int total = L * np;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int l = i / np, k = 2 * (i - l * np);
+      const long long ra = r0 + 2 * l, rb = ra + 1;
+      const float2 z0 = buf[lay(l, k)], m0 = buf[lay(l, k == 0 ? 0 : n - k)];
+      const float2 z1 = buf[lay(l, k + 1)], m1 = buf[lay(l, n - k - 1)];
+      const float4 A = make_float4(0.5f * (z0.x + m0.x), 0.5f * (z0.y - m0.y), 0.5f * (z1.x + m1.x),
+                                   0.5f * (z1.y - m1.y));
+      const float4 B = make_float4(0.5f * (z0.y + m0.y), -0.5f * (z0.x - m0.x), 0.5f * (z1.y + m1.y),
+                                   -0.5f * (z1.x - m1.x));
+      if (k + 1 < nh) {
+        if (ra < d.nrows) *reinterpret_cast<float4*>(S + ra * d.nxp + k) = A;
+        if (rb < d.nrows) *reinterpret_cast<float4*>(S + rb * d.nxp + k) = B;
+      } else {
+        if (ra < d.nrows) S[ra * d.nxp + k] = make_float2(A.x, A.y);
+        if (rb < d.nrows) S[rb * d.nxp + k] = make_float2(B.x, B.y);
+      }
+    }
+    return;
+  }
+  const int n = NC > 0 ? NC : d.nx;
+  const int nh = n / 2 + 1;
   const int total = L * nh;
+#pragma unroll 4
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int l = i / nh, k = i - l * nh;
     const long long ra = r0 + 2 * l, rb = ra + 1;
@@ -242,9 +294,50 @@ __device__ __forceinline__ void sensor_dense(const Sensor& s, int fi, long long 
   sensor_all(s, fi, gi, v);
 }
 
+// ----- 4-wide (16-byte) variants for the compile-time path -----
+__device__ __forceinline__ float4 ld4(const float* p, long long i) { return *reinterpret_cast<const float4*>(p + i); }
+__device__ __forceinline__ void st4(float* p, long long i, float4 v) { *reinterpret_cast<float4*>(p + i) = v; }
+__device__ __forceinline__ float4 map4(const Map& m, long long i) {
+  return m.p ? __ldg(reinterpret_cast<const float4*>(m.p + i)) : make_float4(m.s, m.s, m.s, m.s);
+}
+__device__ __forceinline__ float4 max4(float4 a, float4 b) {
+  return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+}
+__device__ __forceinline__ float4 min4(float4 a, float4 b) {
+  return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
+}
+__device__ __forceinline__ float2 kahan_add(float2 acc, float v) {
+  const float y = v * v - acc.y;
+  const float t = acc.x + y;
+  acc.y = (t - acc.x) - y;
+  acc.x = t;
+  return acc;
+}
+
+// Dense sensors and full-grid reductions for 4 consecutive points.
+__device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long gi, float4 v) {
+  if (fi <= 0) return;
+  if (s.mode == 1) {
+    if (s.raw) st4(s.raw, (long long)(fi - 1) * s.ns + gi, v);
+    if (s.vmax) st4(s.vmax, gi, fi == 1 ? v : max4(ld4(s.vmax, gi), v));
+    if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
+    if (s.rms) {
+      float4* r = reinterpret_cast<float4*>(s.rms + gi);
+      float4 a = (fi == 1) ? make_float4(0.f, 0.f, 0.f, 0.f) : r[0];
+      float4 b = (fi == 1) ? make_float4(0.f, 0.f, 0.f, 0.f) : r[1];
+      float2 t0 = kahan_add(make_float2(a.x, a.y), v.x), t1 = kahan_add(make_float2(a.z, a.w), v.y);
+      float2 t2 = kahan_add(make_float2(b.x, b.y), v.z), t3 = kahan_add(make_float2(b.z, b.w), v.w);
+      r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
+      r[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+    }
+  }
+  if (s.max_all) st4(s.max_all, gi, fi == 1 ? v : max4(ld4(s.max_all, gi), v));
+  if (s.min_all) st4(s.min_all, gi, fi == 1 ? v : min4(ld4(s.min_all, gi), v));
+}
+
 // Sparse sensors (mode 2) of a row tile, values read from the packed buffer.
-__device__ void sensor_sparse_tile(const Sensor& s, int fi, const float2* buf, RowLayout lay,
-                                   const Dims& d, long long r0, int L, int* sh) {
+__device__ void sensor_sparse_tile(const Sensor& s, int fi, const float2* buf, RowLayout lay, const Dims& d,
+                                   long long r0, int L, int* sh) {
   if (s.mode != 2 || fi <= 0) return;
   const long long rend = min(r0 + 2LL * L, d.nrows);
   tile_range(s.idx, s.ns, r0 * d.nx, rend * d.nx, sh);
@@ -261,27 +354,36 @@ __device__ __forceinline__ float src_value(const SparseSource& s, const float* s
   return __ldg(sig + (long long)(t - 1) * s.nrows_sig + row);
 }
 
+template <int NC>
+__device__ __forceinline__ int row_lines(int L) {
+  return NC > 0 ? Tile<NC>::LINES : L;
+}
+
 // ---------------------------------------------------------------------------
 // u update: C2R of the gradient, split-PML momentum update, velocity
 // sources, velocity sensors, R2C of the new velocity.  blockIdx.y = axis.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_x_u(UArgs a, Dims d, FFTPlan plan,
-                                                  const float2* __restrict__ tw_g, int L) {
+template <int NC>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
+                                                           const __grid_constant__ FFTPlan plan,
+                                                           const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
   __shared__ int sh[2];
-  const int nx = d.nx;
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
   const int ax = blockIdx.y;
   const RowLayout lay{row_layout_stride(nx)};
   float2* tw = sm;
   float2* B0 = sm + nx;
-  float2* B1 = B0 + L * lay.ls;
+  float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = (long long)blockIdx.x * 2 * L;
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
-  load_c2r(a.S[ax], B0, lay, d, r0, L);
+  load_c2r<NC>(a.S[ax], B0, lay, d, r0, L);
   __syncthreads();
-  float2* G = fft_lines<true, false>(B0, B1, tw, plan, L, lay);
+  float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
   float2* W = (G == B0) ? B1 : B0;
   float* u = a.u[ax];
   const float* pml = a.pml_sg[ax];
@@ -290,26 +392,67 @@ __global__ void __launch_bounds__(kThreads) k_x_u(UArgs a, Dims d, FFTPlan plan,
   const bool dense_on = ds.field && t <= ds.len;
   const float damp = dense_on ? (ds.sig ? __ldg(ds.sig + t - 1) : 1.f) : 0.f;
   const int total = 2 * L * nx;
-  for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    const int q = i / nx, x = i - q * nx;
-    const long long row = r0 + q;
-    if (row >= d.nrows) {
-      set_comp(G, lay, q, x, 0.f);
-      continue;
+  constexpr bool VEC = NC > 0 && NC % 4 == 0;
+  if constexpr (VEC) {
+    // 4 consecutive points per iteration, 16-byte global accesses
+#pragma unroll 4
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) set_comp(G, lay, q, x + j, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      float4 pm;
+      if (ax == 0) {
+        pm = __ldg(reinterpret_cast<const float4*>(pml + x));
+      } else {
+        const float v = __ldg(pml + (ax == 1 ? (int)(row % d.ny) : (int)(row / d.ny)));
+        pm = make_float4(v, v, v, v);
+      }
+      const float4 rv = map4(rinv, gi);
+      const float4 uo = a.init ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(u, gi);
+      const float4 sv = dense_on ? __ldg(reinterpret_cast<const float4*>(ds.field + gi)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float pmv[4] = {pm.x, pm.y, pm.z, pm.w}, rvv[4] = {rv.x, rv.y, rv.z, rv.w};
+      const float uov[4] = {uo.x, uo.y, uo.z, uo.w}, svv[4] = {sv.x, sv.y, sv.z, sv.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float g = get_comp(G, lay, q, x + j);
+        float un;
+        if (a.init)
+          un = a.dt * rvv[j] * g / 2.f;
+        else
+          un = pmv[j] * (pmv[j] * uov[j] - a.dt * rvv[j] * g);
+        if (dense_on) un = un + damp * svv[j];
+        set_comp(G, lay, q, x + j, un);
+      }
     }
-    const long long gi = row * nx + x;
-    const float g = get_comp(G, lay, q, x);
-    const int y = (int)(row % d.ny), z = (int)(row / d.ny);
-    const int coord = (ax == 0) ? x : ((ax == 1) ? y : z);
-    const float pm = __ldg(pml + coord);
-    const float rv = rinv.at(gi);
-    float un;
-    if (a.init)
-      un = a.dt * rv * g / 2.f;
-    else
-      un = pm * (pm * u[gi] - a.dt * rv * g);
-    if (dense_on) un = un + damp * __ldg(ds.field + gi);
-    set_comp(G, lay, q, x, un);
+  } else {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) {
+        set_comp(G, lay, q, x, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const float g = get_comp(G, lay, q, x);
+      int coord = x;
+      if (ax == 1) coord = (int)(row % d.ny);
+      if (ax == 2) coord = (int)(row / d.ny);
+      const float pm = __ldg(pml + coord);
+      const float rv = rinv.at(gi);
+      float un;
+      if (a.init)
+        un = a.dt * rv * g / 2.f;
+      else
+        un = pm * (pm * u[gi] - a.dt * rv * g);
+      if (dense_on) un = un + damp * __ldg(ds.field + gi);
+      set_comp(G, lay, q, x, un);
+    }
   }
   __syncthreads();
   // sparse velocity sources (dirichlet / additive without correction)
@@ -328,20 +471,35 @@ __global__ void __launch_bounds__(kThreads) k_x_u(UArgs a, Dims d, FFTPlan plan,
     __syncthreads();
   }
   const Sensor& s = a.sens[ax];
-  for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    const int q = i / nx, x = i - q * nx;
-    const long long row = r0 + q;
-    if (row >= d.nrows) continue;
-    const long long gi = row * nx + x;
-    const float v = get_comp(G, lay, q, x);
-    u[gi] = v;
-    sensor_dense(s, fi, gi, v);
+  if constexpr (VEC) {
+#pragma unroll 4
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) continue;
+      const long long gi = row * nx + x;
+      const float4 v = make_float4(get_comp(G, lay, q, x), get_comp(G, lay, q, x + 1), get_comp(G, lay, q, x + 2),
+                                   get_comp(G, lay, q, x + 3));
+      st4(u, gi, v);
+      sensor_dense4(s, fi, gi, v);
+    }
+  } else {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) continue;
+      const long long gi = row * nx + x;
+      const float v = get_comp(G, lay, q, x);
+      u[gi] = v;
+      sensor_dense(s, fi, gi, v);
+    }
   }
   sensor_sparse_tile(s, fi, G, lay, d, r0, L, sh);
   if (a.do_r2c) {
     __syncthreads();
-    float2* F = fft_lines<false, false>(G, W, tw, plan, L, lay);
-    store_r2c(F, a.Sout[ax], lay, d, r0, L);
+    float2* F = tile_fft<NC, false, false>(G, W, tw, plan, L, lay);
+    store_r2c<NC>(F, a.Sout[ax], lay, d, r0, L);
   }
 }
 
@@ -351,40 +509,53 @@ __global__ void __launch_bounds__(kThreads) k_x_u(UArgs a, Dims d, FFTPlan plan,
 // lossless / Stokes EOS (p, sensors, R2C of p) or, for power-law absorption,
 // the local part of p plus the R2C of rho0 * sum(du) and sum(rho).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_x_rho(RhoArgs a, Dims d, FFTPlan plan,
-                                                    const float2* __restrict__ tw_g, int L) {
+template <int NC, int DIM>
+__global__ void __launch_bounds__(Tile<NC>::THREADS, 1) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
   __shared__ int sh[2];
-  const int nx = d.nx, dim = d.dim;
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
+  constexpr int dim = DIM;
   const RowLayout lay{row_layout_stride(nx)};
   float2* tw = sm;
   float2* pool[4];
-  for (int b = 0; b <= dim; ++b) pool[b] = sm + nx + b * L * lay.ls;
+  for (int b = 0; b < 4; ++b) pool[b] = sm + nx + b * L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = (long long)blockIdx.x * 2 * L;
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
-  // inverse x transforms of the three divergence components
+  // inverse x transforms of the divergence components
   float2* D[3] = {nullptr, nullptr, nullptr};
-  bool used[4] = {false, false, false, false};
-  for (int f = 0; f < dim; ++f) {
-    int ia = -1, ib = -1;
-    for (int b = 0; b <= dim; ++b) {
-      if (!used[b]) {
-        if (ia < 0)
-          ia = b;
-        else if (ib < 0)
-          ib = b;
-      }
-    }
-    load_c2r(a.S[f], pool[ia], lay, d, r0, L);
-    __syncthreads();
-    D[f] = fft_lines<true, false>(pool[ia], pool[ib], tw, plan, L, lay);
-    used[(D[f] == pool[ia]) ? ia : ib] = true;
-  }
   float2* Wk = nullptr;
-  for (int b = 0; b <= dim; ++b)
-    if (!used[b]) Wk = pool[b];
+  if constexpr (CT) {
+    _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+      load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L);
+      __syncthreads();
+      D[f] = tile_fft<NC, true, false>(pool[f], nullptr, tw, plan, L, lay);
+    }
+  } else {
+    bool used[4] = {false, false, false, false};
+    _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+      int ia = -1, ib = -1;
+      _Pragma("unroll") for (int b = 0; b <= dim; ++b) {
+        if (!used[b]) {
+          if (ia < 0)
+            ia = b;
+          else if (ib < 0)
+            ib = b;
+        }
+      }
+      load_c2r<NC>(a.S[f], pool[ia], lay, d, r0, L);
+      __syncthreads();
+      D[f] = tile_fft<NC, true, false>(pool[ia], pool[ib], tw, plan, L, lay);
+      used[(D[f] == pool[ia]) ? ia : ib] = true;
+    }
+    _Pragma("unroll") for (int b = 0; b <= dim; ++b)
+      if (!used[b]) Wk = pool[b];
+  }
 
   const bool sp = (a.src.n > 0) && (t <= a.src.len);
   const bool dense_on = a.dsrc.field && t <= a.dsrc.len;
@@ -392,8 +563,91 @@ __global__ void __launch_bounds__(kThreads) k_x_rho(RhoArgs a, Dims d, FFTPlan p
   const int total = 2 * L * nx;
   const bool absorbing = (a.eos == 1);
 
-  // Phase A: rho update (stored to global when sparse sources must be
-  // applied before the equation of state).
+  constexpr bool VEC = NC > 0 && NC % 4 == 0;
+  if (VEC && !sp) {
+    // 4 consecutive points per iteration, 16-byte global accesses
+#pragma unroll 2
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x + j, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const int y = (int)(row % d.ny), z = (int)(row / d.ny);
+      float4 ro[3], pm4[3];
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) ro[f] = ld4(a.rho[f], gi);
+      pm4[0] = __ldg(reinterpret_cast<const float4*>(a.pml[0] + x));
+      {
+        const float vy = __ldg(a.pml[1] + y);
+        pm4[1] = make_float4(vy, vy, vy, vy);
+        if (dim == 3) {
+          const float vz = __ldg(a.pml[2] + z);
+          pm4[2] = make_float4(vz, vz, vz, vz);
+        }
+      }
+      const float4 r0v4 = map4(a.rho0, gi);
+      const float4 c24 = map4(a.c0sq, gi);
+      const float4 bn4 = a.nonlinear ? map4(a.bona, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 ta4 = (a.eos == 2) ? map4(a.tau, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 ds4 = dense_on ? __ldg(reinterpret_cast<const float4*>(a.dsrc.field + gi))
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+      float rn[3][4], outp[4], outq[4], outr[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        auto c = [&](const float4& v) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); };
+        float du[3], rold[3];
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+          du[f] = get_comp(D[f], lay, q, x + j);
+          rold[f] = c(ro[f]);
+        }
+        const float r0v = c(r0v4);
+        float rpr = r0v;
+        if (a.nonlinear) {
+          float rs = rold[0] + rold[1];
+          if (dim == 3) rs += rold[2];
+          rpr = 2.f * rs + r0v;
+        }
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+          const float pm = c(pm4[f]);
+          rn[f][j] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
+          if (dense_on) rn[f][j] = rn[f][j] + damp * c(ds4);
+        }
+        float rsum = rn[0][j] + rn[1][j];
+        if (dim == 3) rsum += rn[2][j];
+        float dsum = du[0] + du[1];
+        if (dim == 3) dsum += du[2];
+        float term = rsum;
+        if (a.eos == 2) term = term + c(ta4) * r0v * dsum;
+        if (a.nonlinear) term = term + c(bn4) * rsum * rsum / (2.f * r0v);
+        outp[j] = c(c24) * term;
+        outq[j] = r0v * dsum;
+        outr[j] = rsum;
+      }
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) st4(a.rho[f], gi, make_float4(rn[f][0], rn[f][1], rn[f][2], rn[f][3]));
+      const float4 pv4 = make_float4(outp[0], outp[1], outp[2], outp[3]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (absorbing) {
+          set_comp(D[0], lay, q, x + j, outq[j]);
+          set_comp(D[1], lay, q, x + j, outr[j]);
+        } else {
+          set_comp(D[0], lay, q, x + j, outp[j]);
+        }
+      }
+      if (absorbing) {
+        st4(a.p_loc, gi, pv4);
+      } else {
+        if (a.p_out) st4(a.p_out, gi, pv4);
+        sensor_dense4(a.sens, fi, gi, pv4);
+      }
+    }
+  } else {
+  // Phase A: rho update (stored to global before the EOS when sparse
+  // sources must be applied first).
   float rnew[3];
   for (int pass = 0; pass < (sp ? 2 : 1); ++pass) {
     if (sp && pass == 1) {
@@ -405,44 +659,42 @@ __global__ void __launch_bounds__(kThreads) k_x_rho(RhoArgs a, Dims d, FFTPlan p
       for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
         const long long gi = __ldg(a.src.idx + j);
         const float v = src_value(a.src, a.src.sig, j, t);
-        for (int f = 0; f < dim; ++f) a.rho[f][gi] = (a.src.mode == 0) ? v : a.rho[f][gi] + v;
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) a.rho[f][gi] = (a.src.mode == 0) ? v : a.rho[f][gi] + v;
       }
       __syncthreads();
     }
+#pragma unroll 2
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
       if (row >= d.nrows) {
-        for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x, 0.f);
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x, 0.f);
         continue;
       }
       const long long gi = row * nx + x;
-      const int y = (int)(row % d.ny), z = (int)(row / d.ny);
       float du[3];
-      for (int f = 0; f < dim; ++f) du[f] = get_comp(D[f], lay, q, x);
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) du[f] = get_comp(D[f], lay, q, x);
       const float r0v = a.rho0.at(gi);
       if (pass == 0) {
         float rold[3];
-        for (int f = 0; f < dim; ++f) rold[f] = a.rho[f][gi];
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) rold[f] = a.rho[f][gi];
         float rpr = r0v;
         if (a.nonlinear) {
           float rs = rold[0] + rold[1];
           if (dim == 3) rs += rold[2];
           rpr = 2.f * rs + r0v;
         }
+        const int y = (int)(row % d.ny), z = (int)(row / d.ny);
         const int coord[3] = {x, y, z};
-        for (int f = 0; f < dim; ++f) {
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
           const float pm = __ldg(a.pml[f] + coord[f]);
           rnew[f] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
           if (dense_on) rnew[f] = rnew[f] + damp * __ldg(a.dsrc.field + gi);
+          a.rho[f][gi] = rnew[f];
         }
-        if (sp) {
-          for (int f = 0; f < dim; ++f) a.rho[f][gi] = rnew[f];
-          continue;
-        }
-        for (int f = 0; f < dim; ++f) a.rho[f][gi] = rnew[f];
+        if (sp) continue;
       } else {
-        for (int f = 0; f < dim; ++f) rnew[f] = a.rho[f][gi];
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) rnew[f] = a.rho[f][gi];
       }
       // equation of state (kspaceFirstOrder3D.m:963-1017)
       float rsum = rnew[0] + rnew[1];
@@ -465,81 +717,125 @@ __global__ void __launch_bounds__(kThreads) k_x_rho(RhoArgs a, Dims d, FFTPlan p
       }
     }
   }
+  }
   __syncthreads();
   if (absorbing) {
-    float2* F = fft_lines<false, false>(D[0], Wk, tw, plan, L, lay);
-    store_r2c(F, a.S_q, lay, d, r0, L);
+    float2* F = tile_fft<NC, false, false>(D[0], Wk, tw, plan, L, lay);
+    store_r2c<NC>(F, a.S_q, lay, d, r0, L);
     __syncthreads();
-    float2* Wk2 = (F == D[0]) ? Wk : D[0];
-    F = fft_lines<false, false>(D[1], Wk2, tw, plan, L, lay);
-    store_r2c(F, a.S_r, lay, d, r0, L);
+    float2* Wk2 = CT ? nullptr : ((F == D[0]) ? Wk : D[0]);
+    F = tile_fft<NC, false, false>(D[1], Wk2, tw, plan, L, lay);
+    store_r2c<NC>(F, a.S_r, lay, d, r0, L);
   } else {
     sensor_sparse_tile(a.sens, fi, D[0], lay, d, r0, L, sh);
     __syncthreads();
-    float2* F = fft_lines<false, false>(D[0], Wk, tw, plan, L, lay);
-    store_r2c(F, a.S_p, lay, d, r0, L);
+    float2* F = tile_fft<NC, false, false>(D[0], Wk, tw, plan, L, lay);
+    store_r2c<NC>(F, a.S_p, lay, d, r0, L);
   }
 }
 
 // ---------------------------------------------------------------------------
 // power-law absorbing EOS: p = p_loc + c0^2 tau A - c0^2 eta B, sensors, R2C.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_x_eos(EosArgs a, Dims d, FFTPlan plan,
-                                                    const float2* __restrict__ tw_g, int L) {
+template <int NC>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_constant__ EosArgs a, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
   __shared__ int sh[2];
-  const int nx = d.nx;
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
   const RowLayout lay{row_layout_stride(nx)};
   float2* tw = sm;
   float2* P0 = sm + nx;
   float2* P1 = P0 + L * lay.ls;
-  float2* P2 = P1 + L * lay.ls;
+  float2* P2 = CT ? nullptr : P1 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = (long long)blockIdx.x * 2 * L;
   const int fi = record_index(a.clk);
-  load_c2r(a.S_a, P0, lay, d, r0, L);
-  __syncthreads();
-  float2* RA = fft_lines<true, false>(P0, P1, tw, plan, L, lay);
-  float2* f1 = (RA == P0) ? P1 : P0;
-  load_c2r(a.S_b, f1, lay, d, r0, L);
-  __syncthreads();
-  float2* RB = fft_lines<true, false>(f1, P2, tw, plan, L, lay);
-  float2* Wk = (RB == f1) ? P2 : f1;
+  float2 *RA, *RB, *Wk;
+  load_c2r<NC>(a.S_a, P0, lay, d, r0, L);
+  if constexpr (CT) {
+    load_c2r<NC>(a.S_b, P1, lay, d, r0, L);
+    __syncthreads();
+    RA = tile_fft<NC, true, false>(P0, nullptr, tw, plan, L, lay);
+    RB = tile_fft<NC, true, false>(P1, nullptr, tw, plan, L, lay);
+    Wk = nullptr;
+  } else {
+    __syncthreads();
+    RA = tile_fft<NC, true, false>(P0, P1, tw, plan, L, lay);
+    float2* f1 = (RA == P0) ? P1 : P0;
+    load_c2r<NC>(a.S_b, f1, lay, d, r0, L);
+    __syncthreads();
+    RB = tile_fft<NC, true, false>(f1, P2, tw, plan, L, lay);
+    Wk = (RB == f1) ? P2 : f1;
+  }
   const int total = 2 * L * nx;
-  for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    const int q = i / nx, x = i - q * nx;
-    const long long row = r0 + q;
-    if (row >= d.nrows) {
-      set_comp(RA, lay, q, x, 0.f);
-      continue;
+  if constexpr (NC > 0 && NC % 4 == 0) {
+#pragma unroll 4
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) set_comp(RA, lay, q, x + j, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const float4 pl = ld4(a.p_loc, gi), ct = map4(a.c2tau, gi), ce = map4(a.c2eta, gi);
+      const float plv[4] = {pl.x, pl.y, pl.z, pl.w}, ctv[4] = {ct.x, ct.y, ct.z, ct.w};
+      const float cev[4] = {ce.x, ce.y, ce.z, ce.w};
+      float pv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        pv[j] = plv[j] + ctv[j] * get_comp(RA, lay, q, x + j) - cev[j] * get_comp(RB, lay, q, x + j);
+        set_comp(RA, lay, q, x + j, pv[j]);
+      }
+      const float4 p4 = make_float4(pv[0], pv[1], pv[2], pv[3]);
+      if (a.p_out) st4(a.p_out, gi, p4);
+      sensor_dense4(a.sens, fi, gi, p4);
     }
-    const long long gi = row * nx + x;
-    const float A = get_comp(RA, lay, q, x);
-    const float B = get_comp(RB, lay, q, x);
-    const float pv = a.p_loc[gi] + a.c2tau.at(gi) * A - a.c2eta.at(gi) * B;
-    set_comp(RA, lay, q, x, pv);
-    if (a.p_out) a.p_out[gi] = pv;
-    sensor_dense(a.sens, fi, gi, pv);
+  } else {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.nrows) {
+        set_comp(RA, lay, q, x, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const float A = get_comp(RA, lay, q, x);
+      const float B = get_comp(RB, lay, q, x);
+      const float pv = a.p_loc[gi] + a.c2tau.at(gi) * A - a.c2eta.at(gi) * B;
+      set_comp(RA, lay, q, x, pv);
+      if (a.p_out) a.p_out[gi] = pv;
+      sensor_dense(a.sens, fi, gi, pv);
+    }
   }
   __syncthreads();
   sensor_sparse_tile(a.sens, fi, RA, lay, d, r0, L, sh);
   __syncthreads();
-  float2* F = fft_lines<false, false>(RA, Wk, tw, plan, L, lay);
-  store_r2c(F, a.S_p, lay, d, r0, L);
+  float2* F = tile_fft<NC, false, false>(RA, Wk, tw, plan, L, lay);
+  store_r2c<NC>(F, a.S_p, lay, d, r0, L);
 }
 
 // ---------------------------------------------------------------------------
 // plain x transforms (setup work, sources with k-space correction)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_x_r2c(const float* __restrict__ f, float2* S, Dims d,
-                                                    FFTPlan plan, const float2* __restrict__ tw_g,
-                                                    int L) {
+template <int NC>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_r2c(const float* __restrict__ f, float2* S, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
-  const int nx = d.nx;
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
   const RowLayout lay{row_layout_stride(nx)};
   float2* tw = sm;
   float2* B0 = sm + nx;
-  float2* B1 = B0 + L * lay.ls;
+  float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = (long long)blockIdx.x * 2 * L;
   const int total = 2 * L * nx;
@@ -549,25 +845,29 @@ __global__ void __launch_bounds__(kThreads) k_x_r2c(const float* __restrict__ f,
     set_comp(B0, lay, q, x, row < d.nrows ? f[row * nx + x] : 0.f);
   }
   __syncthreads();
-  float2* F = fft_lines<false, false>(B0, B1, tw, plan, L, lay);
-  store_r2c(F, S, lay, d, r0, L);
+  float2* F = tile_fft<NC, false, false>(B0, B1, tw, plan, L, lay);
+  store_r2c<NC>(F, S, lay, d, r0, L);
 }
 
 // out = v (accumulate == 0) or out += v
-__global__ void __launch_bounds__(kThreads) k_x_c2r(const float2* __restrict__ S, float* out,
-                                                    int accumulate, Dims d, FFTPlan plan,
-                                                    const float2* __restrict__ tw_g, int L) {
+template <int NC>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_c2r(const float2* __restrict__ S, float* out,
+                                                             int accumulate, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
-  const int nx = d.nx;
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
   const RowLayout lay{row_layout_stride(nx)};
   float2* tw = sm;
   float2* B0 = sm + nx;
-  float2* B1 = B0 + L * lay.ls;
+  float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = (long long)blockIdx.x * 2 * L;
-  load_c2r(S, B0, lay, d, r0, L);
+  load_c2r<NC>(S, B0, lay, d, r0, L);
   __syncthreads();
-  float2* G = fft_lines<true, false>(B0, B1, tw, plan, L, lay);
+  float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
   const int total = 2 * L * nx;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int q = i / nx, x = i - q * nx;
@@ -592,8 +892,8 @@ __global__ void k_scatter(float* f, const int* __restrict__ idx, const int* __re
 }
 
 // rho_i = p0 / (dim c0^2) (kspaceFirstOrder3D.m:1027-1030, 2D.m:915-916)
-__global__ void k_rho_init(float* r0, float* r1, float* r2, const float* __restrict__ p0, Map c0sq,
-                           int dim, long long n) {
+__global__ void k_rho_init(float* r0, float* r1, float* r2, const float* __restrict__ p0, Map c0sq, int dim,
+                           long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const float v = p0[i] / ((float)dim * c0sq.at(i));
@@ -629,75 +929,160 @@ __global__ void k_rms_final(const float2* __restrict__ acc, float* out, long lon
 }
 
 // ---------------------------------------------------------------------------
-// host-side launch helpers
+// host-side launch helpers, dispatching on the transform length
 // ---------------------------------------------------------------------------
-size_t smem_col(int n, int tl, int nbuf) { return sizeof(float2) * ((size_t)n + (size_t)nbuf * tl * n); }
-size_t smem_row(int nx, int L, int nbuf) {
+// Lengths with a compile-time engine; any other 2^a 3^b 5^c length runs on
+// the runtime-plan engine.
+#define KWB_CT_SIZES(X) X(64) X(128) X(256) X(512)
+
+bool ct_supported(int n) {
+#define KWB_CASE(N) \
+  if (n == N) return true;
+  KWB_CT_SIZES(KWB_CASE)
+#undef KWB_CASE
+  return false;
+}
+
+int col_lines(int n, int tl_rt) { return ct_supported(n) ? ct_lines_of(n) : tl_rt; }
+int row_lines_host(int n, int l_rt) { return ct_supported(n) ? ct_lines_of(n) : l_rt; }
+
+static size_t smem_col(int n, int tl, int nbuf) { return sizeof(float2) * ((size_t)n + (size_t)nbuf * tl * n); }
+static size_t smem_row(int nx, int L, int nbuf) {
   return sizeof(float2) * ((size_t)nx + (size_t)nbuf * L * row_layout_stride(nx));
+}
+
+template <class K>
+static void set_smem(K k, size_t sm) {
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+}
+
+#define KWB_DISPATCH(n, CALL)                 \
+  switch (n) {                                \
+    case 64: { constexpr int NC = 64; CALL; } break;   \
+    case 128: { constexpr int NC = 128; CALL; } break; \
+    case 256: { constexpr int NC = 256; CALL; } break; \
+    case 512: { constexpr int NC = 512; CALL; } break; \
+    default: { constexpr int NC = 0; CALL; } break;    \
+  }
+
+template <int NC, bool INV>
+static void col_fft_t(const ColArgs& a0, int nfields, long long nouter, const FFTPlan& plan, const float2* tw,
+                      cudaStream_t st) {
+  ColArgs a = a0;
+  const int tl = NC > 0 ? Tile<NC>::LINES : a.tl;
+  a.tl = tl;
+  dim3 grid((a.ncols + tl - 1) / tl, (unsigned)nouter, nfields);
+  const size_t sm = smem_col(plan.n, tl, NC > 0 ? 1 : 2);
+  set_smem(k_col_fft<NC, INV>, sm);
+  k_col_fft<NC, INV><<<grid, Tile<NC>::THREADS, sm, st>>>(a, plan, tw);
 }
 
 cudaError_t launch_col_fft(bool inv, const ColArgs& a, int nfields, long long nouter, const FFTPlan& plan,
                            const float2* tw, cudaStream_t st) {
-  dim3 grid((a.ncols + a.tl - 1) / a.tl, (unsigned)nouter, nfields);
-  const size_t sm = smem_col(plan.n, a.tl, 2);
   if (inv) {
-    cudaFuncSetAttribute(k_col_fft<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_col_fft<true><<<grid, kThreads, sm, st>>>(a, plan, tw);
+    KWB_DISPATCH(plan.n, (col_fft_t<NC, true>(a, nfields, nouter, plan, tw, st)))
   } else {
-    cudaFuncSetAttribute(k_col_fft<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_col_fft<false><<<grid, kThreads, sm, st>>>(a, plan, tw);
+    KWB_DISPATCH(plan.n, (col_fft_t<NC, false>(a, nfields, nouter, plan, tw, st)))
   }
   return cudaGetLastError();
 }
 
+template <int NC>
+static void fused_t(const FusedArgs& a0, int ninputs, long long nouter, const FFTPlan& plan, const float2* tw,
+                    const SpecTables& T, int dim, cudaStream_t st) {
+  FusedArgs a = a0;
+  const int tl = NC > 0 ? Tile<NC>::LINES : a.tl;
+  a.tl = tl;
+  dim3 grid((a.ncols + tl - 1) / tl, (unsigned)nouter, ninputs);
+  const size_t sm = smem_col(plan.n, tl, NC > 0 ? 2 : 3);
+  set_smem(k_fused_last<NC>, sm);
+  k_fused_last<NC><<<grid, Tile<NC>::THREADS, sm, st>>>(a, plan, tw, T, dim);
+}
+
 cudaError_t launch_fused_last(const FusedArgs& a, int ninputs, long long nouter, const FFTPlan& plan,
                               const float2* tw, const SpecTables& T, int dim, cudaStream_t st) {
-  dim3 grid((a.ncols + a.tl - 1) / a.tl, (unsigned)nouter, ninputs);
-  const size_t sm = smem_col(plan.n, a.tl, 3);
-  cudaFuncSetAttribute(k_fused_last, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_fused_last<<<grid, kThreads, sm, st>>>(a, plan, tw, T, dim);
+  KWB_DISPATCH(plan.n, (fused_t<NC>(a, ninputs, nouter, plan, tw, T, dim, st)))
   return cudaGetLastError();
 }
 
 static inline unsigned row_tiles(const Dims& d, int L) { return (unsigned)((d.nrows + 2 * L - 1) / (2 * L)); }
 
+template <int NC>
+static void x_u_t(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt, cudaStream_t st) {
+  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
+  set_smem(k_x_u<NC>, sm);
+  k_x_u<NC><<<dim3(row_tiles(d, L), d.dim), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+}
+
 cudaError_t launch_x_u(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
                        cudaStream_t st) {
-  const size_t sm = smem_row(d.nx, L, 2);
-  cudaFuncSetAttribute(k_x_u, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_x_u<<<dim3(row_tiles(d, L), d.dim), kThreads, sm, st>>>(a, d, plan, tw, L);
+  KWB_DISPATCH(d.nx, (x_u_t<NC>(a, d, plan, tw, L, st)))
   return cudaGetLastError();
+}
+
+template <int NC>
+static void x_rho_t(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
+                    cudaStream_t st) {
+  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? d.dim : d.dim + 1);
+  if (d.dim == 3) {
+    set_smem(k_x_rho<NC, 3>, sm);
+    k_x_rho<NC, 3><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  } else {
+    set_smem(k_x_rho<NC, 2>, sm);
+    k_x_rho<NC, 2><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  }
 }
 
 cudaError_t launch_x_rho(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
                          cudaStream_t st) {
-  const size_t sm = smem_row(d.nx, L, d.dim + 1);
-  cudaFuncSetAttribute(k_x_rho, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_x_rho<<<row_tiles(d, L), kThreads, sm, st>>>(a, d, plan, tw, L);
+  KWB_DISPATCH(d.nx, (x_rho_t<NC>(a, d, plan, tw, L, st)))
   return cudaGetLastError();
+}
+
+template <int NC>
+static void x_eos_t(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
+                    cudaStream_t st) {
+  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 2 : 3);
+  set_smem(k_x_eos<NC>, sm);
+  k_x_eos<NC><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
 }
 
 cudaError_t launch_x_eos(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
                          cudaStream_t st) {
-  const size_t sm = smem_row(d.nx, L, 3);
-  cudaFuncSetAttribute(k_x_eos, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_x_eos<<<row_tiles(d, L), kThreads, sm, st>>>(a, d, plan, tw, L);
+  KWB_DISPATCH(d.nx, (x_eos_t<NC>(a, d, plan, tw, L, st)))
   return cudaGetLastError();
 }
 
-cudaError_t launch_x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw,
-                         int L, cudaStream_t st) {
-  const size_t sm = smem_row(d.nx, L, 2);
-  cudaFuncSetAttribute(k_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_x_r2c<<<row_tiles(d, L), kThreads, sm, st>>>(f, S, d, plan, tw, L);
+template <int NC>
+static void x_r2c_t(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
+                    cudaStream_t st) {
+  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
+  set_smem(k_x_r2c<NC>, sm);
+  k_x_r2c<NC><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(f, S, d, plan, tw, L);
+}
+
+cudaError_t launch_x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                         cudaStream_t st) {
+  KWB_DISPATCH(d.nx, (x_r2c_t<NC>(f, S, d, plan, tw, L, st)))
   return cudaGetLastError();
+}
+
+template <int NC>
+static void x_c2r_t(const float2* S, float* out, int acc, const Dims& d, const FFTPlan& plan, const float2* tw,
+                    int Lrt, cudaStream_t st) {
+  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
+  set_smem(k_x_c2r<NC>, sm);
+  k_x_c2r<NC><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(S, out, acc, d, plan, tw, L);
 }
 
 cudaError_t launch_x_c2r(const float2* S, float* out, int accumulate, const Dims& d, const FFTPlan& plan,
                          const float2* tw, int L, cudaStream_t st) {
-  const size_t sm = smem_row(d.nx, L, 2);
-  cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_x_c2r<<<row_tiles(d, L), kThreads, sm, st>>>(S, out, accumulate, d, plan, tw, L);
+  KWB_DISPATCH(d.nx, (x_c2r_t<NC>(S, out, accumulate, d, plan, tw, L, st)))
   return cudaGetLastError();
 }
 
@@ -708,21 +1093,20 @@ static inline unsigned ew_blocks(long long n) {
   return (unsigned)b;
 }
 
-cudaError_t launch_scatter(float* f, const int* idx, const int* slot, int n, const float* sig,
-                           int nrows_sig, int t, cudaStream_t st) {
+cudaError_t launch_scatter(float* f, const int* idx, const int* slot, int n, const float* sig, int nrows_sig,
+                           int t, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   k_scatter<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(f, idx, slot, n, sig, nrows_sig, t);
   return cudaGetLastError();
 }
 
-cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim,
-                            long long n, cudaStream_t st) {
+cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim, long long n,
+                            cudaStream_t st) {
   k_rho_init<<<ew_blocks(n), kThreads, 0, st>>>(r0, r1, r2, p0, c0sq, dim, n);
   return cudaGetLastError();
 }
 
-cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& clk, long long n,
-                                cudaStream_t st) {
+cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& clk, long long n, cudaStream_t st) {
   k_record_field<<<ew_blocks(n), kThreads, 0, st>>>(f, s, clk, n);
   return cudaGetLastError();
 }

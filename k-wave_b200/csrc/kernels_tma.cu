@@ -1,0 +1,266 @@
+// Persistent, TMA-fed column passes (the y pass and the fused last-axis
+// operator) for compile-time transform lengths up to 256.
+//
+// Each thread block loops over column tiles (TL adjacent kx columns x the
+// whole line).  Tiles arrive by cp.async.bulk.tensor into a ring of shared
+// memory stages while the previous tile is being transformed, and leave by
+// bulk tensor stores, so the memory system streams continuously instead of
+// stalling on each block's load phase.  The shared-memory tile layout
+// [position][column] is exactly the TMA box layout and the column layout
+// the in-place FFT engine uses.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "fft_ct.cuh"
+#include "kernels.cuh"
+#include "kernels_tma.cuh"
+#include "spec_ops.cuh"
+#include "tma.cuh"
+
+namespace kwb {
+
+template <int NC>
+struct TTile {
+  static constexpr int LINES = ct_lines_of(NC);
+  static constexpr int THREADS = ct_threads_of(NC);
+  static constexpr int ELEMS = LINES * NC;
+  static constexpr unsigned BYTES = ELEMS * sizeof(float2);
+};
+
+__device__ __forceinline__ void tile_coords(int yaxis, int cx, int o, int lines, int& x, int& y, int& z) {
+  x = cx * lines;
+  if (yaxis == 1) {
+    y = 0;
+    z = o;
+  } else {
+    y = o;
+    z = 0;
+  }
+}
+
+template <int NC, bool INV>
+__global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_constant__ ColTmaArgs a,
+                                                                const float2* __restrict__ tw_g) {
+  constexpr int TL = TTile<NC>::LINES;
+  constexpr int E = TTile<NC>::ELEMS;
+  constexpr int ST = 3;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float2* bufs = reinterpret_cast<float2*>(smraw);
+  float2* tw = bufs + ST * E;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + NC);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  for (int i = threadIdx.x; i < NC; i += blockDim.x) tw[i] = tw_g[i];
+  __syncthreads();
+  const int per_field = a.ncx * a.nouter;
+  const int ntiles = a.nfields * per_field;
+  auto coords = [&](int t, int& f, int& x, int& y, int& z) {
+    f = t / per_field;
+    const int r = t - f * per_field;
+    const int o = r / a.ncx;
+    tile_coords(a.yaxis, r - o * a.ncx, o, TL, x, y, z);
+  };
+  auto issue = [&](int t, int s) {
+    int f, x, y, z;
+    coords(t, f, x, y, z);
+    mbar_expect_tx(&bar[s], TTile<NC>::BYTES);
+    tma_load_3d(bufs + s * E, &a.map[f], x, y, z, &bar[s]);
+  };
+  if (threadIdx.x == 0) {
+    for (int f = 0; f < a.nfields; ++f) prefetch_tmap(&a.map[f]);
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  const ColLayout lay{TL};
+  int it = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it % ST;
+    float2* b = bufs + s * E;
+    mbar_wait(&bar[s], (it / ST) & 1, a.err);
+    ct_fft<NC, INV, true, TL>(b, tw, lay);
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int f, x, y, z;
+      coords(t, f, x, y, z);
+      tma_store_3d(&a.map[f], x, y, z, b);
+      bulk_commit();
+      const int t2 = t + 2 * gridDim.x;
+      if (t2 < ntiles) {
+        bulk_wait_read<1>();  // the stage being refilled was stored one tile ago
+        issue(t2, (it + 2) % ST);
+      }
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait<0>();
+}
+
+template <int NC>
+__global__ void __launch_bounds__(TTile<NC>::THREADS, 1) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
+                                                                     const float2* __restrict__ tw_g,
+                                                                     const __grid_constant__ SpecTables T) {
+  constexpr int TL = TTile<NC>::LINES;
+  constexpr int E = TTile<NC>::ELEMS;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float2* inb = reinterpret_cast<float2*>(smraw);  // 2 input stages
+  float2* W = inb + 2 * E;                         // product / inverse-transform buffer
+  float2* tw = W + E;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + NC);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  for (int i = threadIdx.x; i < NC; i += blockDim.x) tw[i] = tw_g[i];
+  __syncthreads();
+  const int per_in = a.ncx * a.nouter;
+  const int ntiles = a.nin * per_in;
+  auto decode = [&](int t, int& g, int& cx, int& o) {
+    g = t / per_in;
+    const int r = t - g * per_in;
+    o = r / a.ncx;
+    cx = r - o * a.ncx;
+  };
+  auto issue = [&](int t, int s) {
+    int g, cx, o, x, y, z;
+    decode(t, g, cx, o);
+    tile_coords(a.yaxis, cx, o, TL, x, y, z);
+    mbar_expect_tx(&bar[s], TTile<NC>::BYTES);
+    tma_load_3d(inb + s * E, &a.in[g], x, y, z, &bar[s]);
+  };
+  if (threadIdx.x == 0) {
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  const ColLayout lay{TL};
+  int it = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it & 1;
+    float2* F = inb + s * E;
+    int g, cx, o;
+    decode(t, g, cx, o);
+    const int x0 = cx * TL;
+    mbar_wait(&bar[s], (it >> 1) & 1, a.err);
+    ct_fft<NC, false, true, TL>(F, tw, lay);
+    for (int q = 0; q < a.fanout; ++q) {
+      const SpecOp op = a.op[g * a.fanout + q];
+#pragma unroll 4
+      for (int i = threadIdx.x; i < E; i += blockDim.x) {
+        const int l = i % TL, p = i / TL;
+        const int ix = min(x0 + l, a.ncols - 1);
+        const int iy = (a.dim == 3) ? o : p;
+        const int iz = (a.dim == 3) ? p : 0;
+        W[i] = c_mul(F[i], eval_op(op, T, a.dim, ix, iy, iz));
+      }
+      __syncthreads();
+      ct_fft<NC, true, true, TL>(W, tw, lay);
+      float2* dst = a.outp[g * a.fanout + q] + (long long)o * a.ostride + x0;
+#pragma unroll 4
+      for (int i = threadIdx.x; i < E; i += blockDim.x) {
+        const int l = i % TL, p = i / TL;
+        if (x0 + l < a.ncols) dst[p * a.lstride + l] = W[i];
+      }
+      __syncthreads();
+    }
+    // F is consumed: refill this input stage with the tile two ahead
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int t2 = t + 2 * gridDim.x;
+      if (t2 < ntiles) issue(t2, s);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static bool get_encoder() {
+  if (g_encode) return true;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+    return false;
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return true;
+}
+
+bool tma_supported(int n) { return n == 64 || n == 128 || n == 256; }
+
+// Tensor map over a half-spectrum buffer [nz][ny][nxp] (8-byte elements),
+// box {lines, ny or 1, 1 or nz} for transforms along y (yaxis 1) or z (2).
+bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n) {
+  if (!get_encoder()) return false;
+  const int lines = ct_lines_of(n);
+  cuuint64_t dims[3] = {(cuuint64_t)d.nxp, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
+  cuuint64_t strides[2] = {(cuuint64_t)d.nxp * 8, (cuuint64_t)d.nxp * d.ny * 8};
+  cuuint32_t box[3] = {(cuuint32_t)lines, yaxis == 1 ? (cuuint32_t)d.ny : 1u, yaxis == 2 ? (cuuint32_t)d.nz : 1u};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+static int g_num_sms = 0;
+static int num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return g_num_sms;
+}
+
+template <int NC, bool INV>
+static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t st) {
+  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 3 * sizeof(uint64_t);
+  auto k = k_col_tma<NC, INV>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
+  const int ntiles = a.nfields * a.ncx * a.nouter;
+  const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
+  k<<<grid, TTile<NC>::THREADS, sm, st>>>(a, tw);
+  return cudaGetLastError();
+}
+
+template <int NC>
+static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
+  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t);
+  auto k = k_fused_tma<NC>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
+  const int ntiles = a.nin * a.ncx * a.nouter;
+  const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
+  k<<<grid, TTile<NC>::THREADS, sm, st>>>(a, tw, T);
+  return cudaGetLastError();
+}
+
+int tma_lines(int n) { return ct_lines_of(n); }
+
+cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* tw, cudaStream_t st) {
+  switch (n) {
+    case 64: return inv ? col_tma_t<64, true>(a, tw, st) : col_tma_t<64, false>(a, tw, st);
+    case 128: return inv ? col_tma_t<128, true>(a, tw, st) : col_tma_t<128, false>(a, tw, st);
+    case 256: return inv ? col_tma_t<256, true>(a, tw, st) : col_tma_t<256, false>(a, tw, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_fused_tma(int n, const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
+  switch (n) {
+    case 64: return fused_tma_t<64>(a, tw, T, st);
+    case 128: return fused_tma_t<128>(a, tw, T, st);
+    case 256: return fused_tma_t<256>(a, tw, T, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace kwb

@@ -1,0 +1,30 @@
+// Argument blocks of the TMA-fed column kernels.
+#pragma once
+#include <cuda.h>
+
+#include "kernels.cuh"
+
+namespace kwb {
+
+struct ColTmaArgs {
+  CUtensorMap map[4];  // one per field; box {LINES, N, 1} (y pass) or {LINES, 1, N} (last axis)
+  int nfields;
+  int ncx;      // column tiles along kx
+  int nouter;   // outer extent (z for the y pass, y for the 3D last axis)
+  int yaxis;    // 1: the transformed axis is the tensor's y dimension, 2: z
+  int* err;
+};
+
+struct FusedTmaArgs {
+  CUtensorMap in[3];
+  CUtensorMap out[9];
+  SpecOp op[9];
+  float2* outp[9];      // output buffers (written with plain stores)
+  long long lstride;    // element stride along the transformed axis
+  long long ostride;    // stride of the outer index
+  int nin, fanout, ncx, nouter, yaxis, dim;
+  int ncols;  // valid kx columns (nx / 2 + 1)
+  int* err;
+};
+
+}  // namespace kwb

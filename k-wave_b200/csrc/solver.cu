@@ -15,6 +15,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -50,6 +51,11 @@ cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& cl
                                 cudaStream_t st);
 cudaError_t launch_advance(int* t, cudaStream_t st);
 cudaError_t launch_rms_final(const float2* acc, float* out, long long n, float inv_n, cudaStream_t st);
+bool tma_supported(int n);
+int tma_lines(int n);
+bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n);
+cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* tw, cudaStream_t st);
+cudaError_t launch_fused_tma(int n, const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st);
 
 static void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -192,7 +198,7 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   d.nz = (int)in->Nz;
   d.dim = (in->Nz == 1) ? 2 : 3;
   d.nxh = d.nx / 2 + 1;
-  d.nxp = (d.nxh + 15) / 16 * 16;
+  d.nxp = (d.nxh + 31) / 32 * 32;  // whole TMA column tiles: no box leaves the buffer
   d.nrows = (long long)d.ny * d.nz;
   d.npts = (long long)d.nx * d.nrows;
   if (d.npts >= (1LL << 31)) throw KwError(KW_ERR_UNSUPPORTED, "grids above 2^31 points are not supported");
@@ -336,6 +342,17 @@ void Session::setup(const kw_input* in, const kw_options* o) {
     S_buf[s].alloc(sb);
     ck(cudaMemsetAsync(S_buf[s].p, 0, sb, st), "memset");
   }
+  err_buf.alloc(sizeof(int));
+  ck(cudaMemsetAsync(err_buf.p, 0, sizeof(int), st), "memset");
+  // TMA-fed column passes for the compile-time lengths they support
+  const char* no_tma = std::getenv("KWAVE_B200_NO_TMA");
+  const bool tma_ok = !(no_tma && no_tma[0] == '1');
+  use_tma[1] = tma_ok && tma_supported(d.ny);
+  use_tma[2] = tma_ok && d.dim == 3 && tma_supported(d.nz);
+  for (int s = 0; s < 4; ++s) {
+    if (use_tma[1] && !make_spec_map(&map_y[s], S_buf[s].p, d, 1, d.ny)) use_tma[1] = false;
+    if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;
+  }
   if (eos == 1) ploc_buf.alloc(fb);
   if (opt.p_final) {
     p_buf.alloc(fb);
@@ -470,47 +487,97 @@ void Session::corrected_source(float* out, const int* idx, const int* slot, int 
   ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, st), "scatter");
   float2* S = (float2*)S_buf[3].p;
   ck(launch_x_r2c(out, S, d, plan[0], twd[0], rowL, st), "x_r2c");
-  run_spectral({S}, {S}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
+  run_spectral({3}, {3}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
   ck(launch_x_c2r(S, out, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
 }
 
-// y passes (3D) around the fused last-axis operator.  `ins` are x-transformed
-// half spectra; outputs are left x-transformed (ready for the row kernels).
-void Session::run_spectral(std::vector<float2*> ins, std::vector<float2*> outs, std::vector<SpecOp> ops,
-                           int fanout) {
+// y passes (3D) around the fused last-axis operator.  `ins` / `outs` index
+// the half-spectrum work buffers, which hold x-transformed data on entry
+// and on exit (ready for the row kernels).
+void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout) {
   const int nin = (int)ins.size();
+  const int nout = (int)outs.size();
+  const int last = d.dim - 1;
+  const int ns[3] = {d.nx, d.ny, d.nz};
+  auto Sp = [&](int i) { return (float2*)S_buf[i].p; };
   if (d.dim == 3) {
-    ColArgs ca{};
-    for (int i = 0; i < nin; ++i) ca.buf[i] = ins[i];
-    ca.ncols = d.nxh;
-    ca.lstride = d.nxp;
-    ca.ostride = (long long)d.nxp * d.ny;
-    ca.tl = col_tl[1];
-    ck(launch_col_fft(false, ca, nin, d.nz, plan[1], twd[1], st), "col_fft fwd");
+    if (use_tma[1]) {
+      ColTmaArgs ca;
+      std::memset(&ca, 0, sizeof(ca));
+      for (int i = 0; i < nin; ++i) ca.map[i] = map_y[ins[i]];
+      ca.nfields = nin;
+      ca.ncx = (d.nxh + tma_lines(d.ny) - 1) / tma_lines(d.ny);
+      ca.nouter = d.nz;
+      ca.yaxis = 1;
+      ca.err = (int*)err_buf.p;
+      ck(launch_col_tma(false, d.ny, ca, twd[1], st), "col_tma fwd");
+    } else {
+      ColArgs ca{};
+      for (int i = 0; i < nin; ++i) ca.buf[i] = Sp(ins[i]);
+      ca.ncols = d.nxh;
+      ca.lstride = d.nxp;
+      ca.ostride = (long long)d.nxp * d.ny;
+      ca.tl = col_tl[1];
+      ck(launch_col_fft(false, ca, nin, d.nz, plan[1], twd[1], st), "col_fft fwd");
+    }
     ++launches_;
   }
-  const int last = d.dim - 1;
-  FusedArgs fa{};
-  for (int i = 0; i < nin; ++i) fa.in[i] = ins[i];
-  for (size_t i = 0; i < outs.size(); ++i) {
-    fa.out[i] = outs[i];
-    fa.op[i] = ops[i];
+  if (use_tma[last]) {
+    FusedTmaArgs fa;
+    std::memset(&fa, 0, sizeof(fa));
+    const CUtensorMap* maps = (d.dim == 3) ? map_z : map_y;
+    for (int i = 0; i < nin; ++i) fa.in[i] = maps[ins[i]];
+    for (int i = 0; i < nout; ++i) {
+      fa.out[i] = maps[outs[i]];
+      fa.outp[i] = Sp(outs[i]);
+      fa.op[i] = ops[i];
+    }
+    fa.lstride = (long long)d.nxp * (d.dim == 3 ? d.ny : 1);
+    fa.ostride = d.nxp;
+    fa.nin = nin;
+    fa.fanout = fanout;
+    fa.ncx = (d.nxh + tma_lines(ns[last]) - 1) / tma_lines(ns[last]);
+    fa.nouter = (d.dim == 3) ? d.ny : 1;
+    fa.yaxis = (d.dim == 3) ? 2 : 1;
+    fa.dim = d.dim;
+    fa.ncols = d.nxh;
+    fa.err = (int*)err_buf.p;
+    ck(launch_fused_tma(ns[last], fa, twd[last], T, st), "fused_tma");
+  } else {
+    FusedArgs fa{};
+    for (int i = 0; i < nin; ++i) fa.in[i] = Sp(ins[i]);
+    for (int i = 0; i < nout; ++i) {
+      fa.out[i] = Sp(outs[i]);
+      fa.op[i] = ops[i];
+    }
+    fa.fanout = fanout;
+    fa.ncols = d.nxh;
+    fa.lstride = (long long)d.nxp * (d.dim == 3 ? d.ny : 1);
+    fa.ostride = d.nxp;
+    fa.tl = col_tl[last];
+    ck(launch_fused_last(fa, nin, d.dim == 3 ? d.ny : 1, plan[last], twd[last], T, d.dim, st), "fused_last");
   }
-  fa.fanout = fanout;
-  fa.ncols = d.nxh;
-  fa.lstride = (long long)d.nxp * (d.dim == 3 ? d.ny : 1);
-  fa.ostride = d.nxp;
-  fa.tl = col_tl[last];
-  ck(launch_fused_last(fa, nin, d.dim == 3 ? d.ny : 1, plan[last], twd[last], T, d.dim, st), "fused_last");
   ++launches_;
   if (d.dim == 3) {
-    ColArgs ca{};
-    for (size_t i = 0; i < outs.size(); ++i) ca.buf[i] = outs[i];
-    ca.ncols = d.nxh;
-    ca.lstride = d.nxp;
-    ca.ostride = (long long)d.nxp * d.ny;
-    ca.tl = col_tl[1];
-    ck(launch_col_fft(true, ca, (int)outs.size(), d.nz, plan[1], twd[1], st), "col_fft inv");
+    if (use_tma[1]) {
+      ColTmaArgs ca;
+      std::memset(&ca, 0, sizeof(ca));
+      for (int i = 0; i < nout; ++i) ca.map[i] = map_y[outs[i]];
+      ca.nfields = nout;
+      ca.ncx = (d.nxh + tma_lines(d.ny) - 1) / tma_lines(d.ny);
+      ca.nouter = d.nz;
+      ca.yaxis = 1;
+      ca.err = (int*)err_buf.p;
+      ck(launch_col_tma(true, d.ny, ca, twd[1], st), "col_tma inv");
+    } else {
+      ColArgs ca{};
+      for (int i = 0; i < nout; ++i) ca.buf[i] = Sp(outs[i]);
+      ca.ncols = d.nxh;
+      ca.lstride = d.nxp;
+      ca.ostride = (long long)d.nxp * d.ny;
+      ca.tl = col_tl[1];
+      ck(launch_col_fft(true, ca, nout, d.nz, plan[1], twd[1], st), "col_fft inv");
+    }
     ++launches_;
   }
 }
@@ -635,13 +702,13 @@ void Session::enqueue_init() {
   float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
   ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
   ++launches_;
-  std::vector<float2*> outs;
+  std::vector<int> outs;
   std::vector<SpecOp> ops;
   for (int a = 0; a < d.dim; ++a) {
-    outs.push_back(S[a + 1]);
+    outs.push_back(a + 1);
     ops.push_back(SpecOp{OP_GRAD_POS, a});
   }
-  run_spectral({S[0]}, outs, ops, d.dim);
+  run_spectral({0}, outs, ops, d.dim);
   UArgs ua = u_args(S);
   ua.init = 1;
   ua.do_r2c = 0;
@@ -681,36 +748,36 @@ void Session::enqueue_step() {
   } else {
     float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
     // (1) momentum: grad p -> u (kspaceFirstOrder3D.m:790-884)
-    std::vector<float2*> outs;
+    std::vector<int> outs;
     std::vector<SpecOp> ops;
     for (int a = 0; a < d.dim; ++a) {
-      outs.push_back(S[a + 1]);
+      outs.push_back(a + 1);
       ops.push_back(SpecOp{OP_GRAD_POS, a});
     }
-    run_spectral({S[0]}, outs, ops, d.dim);
+    run_spectral({0}, outs, ops, d.dim);
     if (u_many_additive) {
       for (int a = 0; a < d.dim; ++a)
         if (udense[a].field && (int)t <= u_len[a]) {
           // S[0] is free here: the gradient has been taken
           corrected_source_into((float*)ufield_buf[a].p, (const int*)usrc_idx.p, (const int*)usrc_slot.p, u_nsrc,
-                                usig_d[a], u_nsig, (int)t, S[0]);
+                                usig_d[a], u_nsig, (int)t, 0);
         }
     }
     UArgs ua = u_args(S);
     ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u");
     ++launches_;
     // (2) mass conservation: div u -> rho, EOS (:905-1017)
-    std::vector<float2*> ins2, outs2;
+    std::vector<int> ins2, outs2;
     std::vector<SpecOp> ops2;
     for (int a = 0; a < d.dim; ++a) {
-      ins2.push_back(S[a + 1]);
-      outs2.push_back(S[a + 1]);
+      ins2.push_back(a + 1);
+      outs2.push_back(a + 1);
       ops2.push_back(SpecOp{OP_GRAD_NEG, a});
     }
     run_spectral(ins2, outs2, ops2, 1);
     if (p_many_additive && (int)t <= p_len)
       corrected_source_into((float*)psrc_field.p, (const int*)psrc_idx.p, (const int*)psrc_slot.p, p_nsrc,
-                            (const float*)psrc_sig.p, p_nsig, (int)t, S[0]);
+                            (const float*)psrc_sig.p, p_nsig, (int)t, 0);
     RhoArgs ra{};
     for (int a = 0; a < d.dim; ++a) {
       ra.S[a] = S[a + 1];
@@ -741,7 +808,7 @@ void Session::enqueue_step() {
     ++launches_;
     if (eos == 1) {
       // (3) power-law absorption and dispersion (:970-977)
-      run_spectral({S[1], S[2]}, {S[1], S[2]}, {SpecOp{OP_NABLA1, 0}, SpecOp{OP_NABLA2, 0}}, 1);
+      run_spectral({1, 2}, {1, 2}, {SpecOp{OP_NABLA1, 0}, SpecOp{OP_NABLA2, 0}}, 1);
       EosArgs ea{};
       ea.S_a = S[1];
       ea.S_b = S[2];
@@ -763,11 +830,12 @@ void Session::enqueue_step() {
 
 // corrected source field for "many" signals, using `work` as spectral scratch
 void Session::corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
-                                    int nrows_sig, int t, float2* work) {
+                                    int nrows_sig, int t, int work_i) {
+  float2* work = (float2*)S_buf[work_i].p;
   ck(cudaMemsetAsync(out, 0, sizeof(float) * d.npts, st), "memset");
   ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, st), "scatter");
   ck(launch_x_r2c(out, work, d, plan[0], twd[0], rowL, st), "x_r2c");
-  run_spectral({work}, {work}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
+  run_spectral({work_i}, {work_i}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
   ck(launch_x_c2r(work, out, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
   launches_ += 4;
 }
@@ -789,7 +857,12 @@ float Session::elapsed_ms() {
   return ms;
 }
 
-void Session::sync() { ck(cudaStreamSynchronize(st), "sync"); }
+void Session::sync() {
+  ck(cudaStreamSynchronize(st), "sync");
+  int e = 0;
+  ck(cudaMemcpy(&e, err_buf.p, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+  if (e) throw KwError(KW_ERR_CUDA, "a device-side wait timed out (error " + std::to_string(e) + ")");
+}
 
 static void d2h(float* dst, const void* src, size_t n, cudaStream_t st) {
   if (dst && src && n) ck(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost, st), "d2h");
@@ -839,7 +912,7 @@ Session::~Session() {
 size_t Session::device_bytes_estimate(const kw_input* in, const kw_options* o) {
   const size_t n = (size_t)(in->Nx * in->Ny * in->Nz);
   const size_t dim = in->Nz == 1 ? 2 : 3;
-  const size_t nxp = ((in->Nx / 2 + 1) + 15) / 16 * 16;
+  const size_t nxp = ((in->Nx / 2 + 1) + 31) / 32 * 32;
   size_t b = 4 * 8 * nxp * in->Ny * in->Nz + 2 * dim * 4 * n;  // spectra, u, rho
   b += 4 * n * (2 + dim);                                       // medium maps
   return b;

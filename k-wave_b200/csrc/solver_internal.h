@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "kernels_tma.cuh"
 #include "kwave_b200.h"
 
 namespace kwb {
@@ -51,8 +52,8 @@ class Session {
   void corrected_source(float* out, const int* idx, const int* slot, int n, const float* sig, int nrows_sig,
                         int t);
   void corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
-                             int nrows_sig, int t, float2* work);
-  void run_spectral(std::vector<float2*> ins, std::vector<float2*> outs, std::vector<SpecOp> ops, int fanout);
+                             int nrows_sig, int t, int work_i);
+  void run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout);
   void enqueue_init();
   void enqueue_step();
   UArgs u_args(float2* const* S);
@@ -80,7 +81,10 @@ class Session {
   DevBuf c0sq_buf, rho0_buf, rinv_buf[3], bona_buf, c2tau_buf, c2eta_buf;
   Map c0sq_m{}, rho0_m{}, rinv_m[3]{}, bona_m{}, c2tau_m{}, c2eta_m{}, tau_m{};
   // fields
-  DevBuf u_buf[3], rho_buf[3], S_buf[4], ploc_buf, p_buf, p0_buf, clock_buf;
+  DevBuf u_buf[3], rho_buf[3], S_buf[4], ploc_buf, p_buf, p0_buf, clock_buf, err_buf;
+  // TMA tensor maps over the half-spectrum buffers (y pass / z pass)
+  bool use_tma[3]{false, false, false};
+  CUtensorMap map_y[4], map_z[4];
   Clock clk{};
   // sources
   SparseSource psrc{}, usrc{};

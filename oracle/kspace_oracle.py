@@ -172,13 +172,17 @@ def cuboid_sizes(corners):
 # the time loop
 # ---------------------------------------------------------------------------
 
-def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers=-1):
+def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers=-1, on_step=None,
+             max_steps=None):
     """Run the fluid time loop (``kspaceFirstOrder3D.m:767-1206``,
     ``kspaceFirstOrder2D.m:710-1042``) on HDF5-file-level inputs.
 
     Returns a dict of outputs in the layout of the drop-in binary's output
     file: time series as (Ns, Nt_rec), per-point reductions as (Ns,),
-    ``*_all`` / ``*_final`` on the full grid (PML included)."""
+    ``*_all`` / ``*_final`` on the full grid (PML included).
+
+    ``on_step(t_index)`` is called after each step and ``max_steps`` stops
+    the loop early (used to time a bounded sample of a long run)."""
     record = set(record)
     for r in record:
         if r not in RECORD_KEYS:
@@ -303,6 +307,8 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
         return col[0] if col.shape[0] == 1 else col
 
     for t_index in range(1, Nt + 1):
+        if max_steps is not None and t_index > max_steps:
+            break
         t = t_index - 1
         # momentum conservation (kspaceFirstOrder3D.m:790-801)
         for i in range(dim):
@@ -402,6 +408,8 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
                 out["p_max_all"] = p.copy() if fi == 1 else np.maximum(out["p_max_all"], p)
             if "p_min_all" in record:
                 out["p_min_all"] = p.copy() if fi == 1 else np.minimum(out["p_min_all"], p)
+        if on_step is not None:
+            on_step(t_index)
     if "p_final" in record:
         out["p_final"] = p
     if "u_final" in record:

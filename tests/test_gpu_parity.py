@@ -146,3 +146,33 @@ def test_output_sizes_and_errors():
     bad["Nx"] = 7 * 8
     with pytest.raises(_lib.KwaveError):
         _solve(bad, record)
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (128, 64, 64), (64, 128, 128)])
+def test_3d_compile_time_sizes_het_absorbing(shape):
+    """Grid edges served by the compile-time FFT engine."""
+    inp, record, start, _ = case_3d_het(n=shape, nt=30, record=("p", "p_max", "p_rms", "u", "p_final"))
+    _check(inp, record, TOL)
+
+
+def test_2d_compile_time_sizes():
+    inp, record, start, _ = case_2d_p0(n=(128, 256), nt=60, record=("p", "p_max", "u", "p_final", "u_final"))
+    _check(inp, record, TOL_LOSSLESS)
+
+
+def test_2d_nonlinear_absorbing_512():
+    from kwave.simulation import prepare
+    from kwave.utils import KWaveGrid, make_disc
+
+    n = (512, 64)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    kg.set_time(40, 0.3e-4 / 1600)
+    rng = np.random.default_rng(11)
+    c = 1500 + 30 * rng.standard_normal(n)
+    medium = {"sound_speed": c, "density": 1000.0, "alpha_coeff": 0.5, "alpha_power": 1.3, "BonA": 5.0}
+    p0 = 1e5 * make_disc(n[0], n[1], 256, 32, 6)
+    mask = np.zeros(n)
+    mask[::17, ::9] = 1
+    inp, record, start, _ = prepare(kg, medium, {"p0": p0}, {"mask": mask, "record": ["p", "p_rms", "u_max"]},
+                                    pml_size=10)
+    _check(inp, record, TOL)
