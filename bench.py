@@ -51,11 +51,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_input(n, nt):
+def build_input(n, nt, shape=None):
     from kwave.simulation import prepare
     from kwave.workloads import het_absorbing_3d
 
-    kg, medium, source, sensor = het_absorbing_3d(n=n, nt=nt)
+    kg, medium, source, sensor = het_absorbing_3d(n=n, nt=nt, shape=shape)
     inp, record, start, _ = prepare(kg, medium, source, sensor)
     return inp, record, start
 
@@ -211,6 +211,7 @@ def main():
     ap.add_argument("--nt", type=int, default=1200)
     ap.add_argument("--e2e-reps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default=None, help="Nx,Ny,Nz for a smaller profiling case (default n^3)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -235,13 +236,14 @@ def main():
 
     from kwave import _lib
 
-    inp, record, start = build_input(args.n, args.nt)
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else None
+    inp, record, start = build_input(args.n, args.nt, shape)
     nt_needed = args.warmup + args.steps
     sess_inp = dict(inp)
     if nt_needed > int(inp["Nt"]):
         sess_inp["Nt"] = nt_needed
     pinned = pin_inputs(sess_inp)
-    npts = args.n ** 3
+    npts = int(inp["Nx"]) * int(inp["Ny"]) * int(inp["Nz"])
 
     # ----- device-resident timing -----
     sess = _lib.Session(pinned, record=record, start_index=start, device=local)
@@ -284,12 +286,12 @@ def main():
 
     peak, peak_kind = peaks()
     achieved = B_ALG * npts / (ms_per_step / 1e3) / 1e9
-    traffic = traffic_per_step(args.n)
+    traffic = traffic_per_step(args.n) if not args.shape else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "Nt": int(inp["Nt"]),
+        "config": {"workload": WORKLOAD, "grid": [int(inp["Nx"]), int(inp["Ny"]), int(inp["Nz"])], "Nt": int(inp["Nt"]),
                    "parallelism": f"replicas{world}", "l2": "working set 1.1 GB > 126 MB L2, no flush needed"},
         "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes(inp), "d2h_bytes_per_step": d2h,
                  "note": f"one e2e step = one whole {int(inp['Nt'])}-step solve via kw_solve, pinned host buffers"}

@@ -115,6 +115,42 @@ __device__ __forceinline__ void ct_stage(float2* buf, const float2* __restrict__
   __syncthreads();
 }
 
+// One stage with caller-supplied element access: ld(l, pos) returns the
+// input element, st(l, pos, v) stores an output element.  No barriers: the
+// caller synchronises (between the loads and stores when they alias, and
+// before the outputs are read).
+template <int N, int STAGE, bool INV, class LD, class ST>
+__device__ __forceinline__ void ct_stage_io(const float2* __restrict__ tw, int l, int tid, LD ld, ST st) {
+  constexpr int R = ct_radix(N, STAGE);
+  constexpr int NS = ct_ns(N, STAGE);
+  constexpr int NR = N / R;
+  constexpr int T = Ct<N>::T;
+  constexpr int NB = (NR + T - 1) / T;
+  constexpr int TWS = N / (NS * R);
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = tid + i * T;
+    if (NR % T == 0 || j < NR) {
+      float2 v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = ld(l, j + r * NR);
+      const int k = j % NS;
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = tw[k * r * TWS];
+          if (INV) w.y = -w.y;
+          v[r] = c_mul(v[r], w);
+        }
+      }
+      dft<R, INV>(v);
+      const int idx = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) st(l, idx + r * NS, v[r]);
+    }
+  }
+}
+
 template <int N, int STAGE, bool INV, class L>
 __device__ __forceinline__ void ct_stages(float2* buf, const float2* __restrict__ tw, int l, int tid, L lay) {
   if constexpr (STAGE < Ct<N>::S) {

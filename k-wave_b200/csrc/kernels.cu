@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
 // the local part of p plus the R2C of rho0 * sum(du) and sum(rho).
 // ---------------------------------------------------------------------------
 template <int NC, int DIM>
-__global__ void __launch_bounds__(Tile<NC>::THREADS, 1) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
+__global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
@@ -531,11 +531,13 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 1) k_x_rho(const __grid_con
   float2* D[3] = {nullptr, nullptr, nullptr};
   float2* Wk = nullptr;
   if constexpr (CT) {
-    _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+#pragma unroll 1
+    for (int f = 0; f < dim; ++f) {
       load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L);
       __syncthreads();
-      D[f] = tile_fft<NC, true, false>(pool[f], nullptr, tw, plan, L, lay);
+      tile_fft<NC, true, false>(pool[f], nullptr, tw, plan, L, lay);
     }
+    _Pragma("unroll") for (int f = 0; f < dim; ++f) D[f] = pool[f];
   } else {
     bool used[4] = {false, false, false, false};
     _Pragma("unroll") for (int f = 0; f < dim; ++f) {
@@ -720,12 +722,21 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 1) k_x_rho(const __grid_con
   }
   __syncthreads();
   if (absorbing) {
-    float2* F = tile_fft<NC, false, false>(D[0], Wk, tw, plan, L, lay);
-    store_r2c<NC>(F, a.S_q, lay, d, r0, L);
-    __syncthreads();
-    float2* Wk2 = CT ? nullptr : ((F == D[0]) ? Wk : D[0]);
-    F = tile_fft<NC, false, false>(D[1], Wk2, tw, plan, L, lay);
-    store_r2c<NC>(F, a.S_r, lay, d, r0, L);
+    if constexpr (CT) {
+#pragma unroll 1
+      for (int f = 0; f < 2; ++f) {
+        if (f) __syncthreads();
+        tile_fft<NC, false, false>(D[f], nullptr, tw, plan, L, lay);
+        store_r2c<NC>(D[f], f == 0 ? a.S_q : a.S_r, lay, d, r0, L);
+      }
+    } else {
+      float2* F = tile_fft<NC, false, false>(D[0], Wk, tw, plan, L, lay);
+      store_r2c<NC>(F, a.S_q, lay, d, r0, L);
+      __syncthreads();
+      float2* Wk2 = (F == D[0]) ? Wk : D[0];
+      F = tile_fft<NC, false, false>(D[1], Wk2, tw, plan, L, lay);
+      store_r2c<NC>(F, a.S_r, lay, d, r0, L);
+    }
   } else {
     sensor_sparse_tile(a.sens, fi, D[0], lay, d, r0, L, sh);
     __syncthreads();
@@ -759,8 +770,10 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_consta
   if constexpr (CT) {
     load_c2r<NC>(a.S_b, P1, lay, d, r0, L);
     __syncthreads();
-    RA = tile_fft<NC, true, false>(P0, nullptr, tw, plan, L, lay);
-    RB = tile_fft<NC, true, false>(P1, nullptr, tw, plan, L, lay);
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) tile_fft<NC, true, false>(f ? P1 : P0, nullptr, tw, plan, L, lay);
+    RA = P0;
+    RB = P1;
     Wk = nullptr;
   } else {
     __syncthreads();

@@ -98,12 +98,18 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
   if (threadIdx.x == 0) bulk_wait<0>();
 }
 
-template <int NC>
-__global__ void __launch_bounds__(TTile<NC>::THREADS, 1) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
+// Operator classes of the fused kernel: one instantiation per class keeps
+// only that operator's arithmetic in the kernel body.
+enum FusedClass { FC_GRAD = 0, FC_NABLA = 1, FC_SRCK = 2 };
+
+template <int NC, int CLS>
+__global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
                                                                      const float2* __restrict__ tw_g,
                                                                      const __grid_constant__ SpecTables T) {
   constexpr int TL = TTile<NC>::LINES;
   constexpr int E = TTile<NC>::ELEMS;
+  constexpr int TH = TTile<NC>::THREADS;
+  static_assert(Ct<NC>::S == 2, "the fused last-axis kernel assumes a two-stage plan");
   extern __shared__ __align__(128) unsigned char smraw[];
   float2* inb = reinterpret_cast<float2*>(smraw);  // 2 input stages
   float2* W = inb + 2 * E;                         // product / inverse-transform buffer
@@ -136,6 +142,9 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 1) k_fused_tma(const __gri
     if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
   }
   const ColLayout lay{TL};
+  // the line mapping fixes this thread's column (kx) for every pass
+  const int l = threadIdx.x % TL, tid = threadIdx.x / TL;
+  const float* kl2 = (a.dim == 3) ? T.k2[2] : T.k2[1];
   int it = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -143,26 +152,53 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 1) k_fused_tma(const __gri
     int g, cx, o;
     decode(t, g, cx, o);
     const int x0 = cx * TL;
+    const int ix = min(x0 + l, a.ncols - 1);
+    const float kxy2 = __ldg(T.k2[0] + ix) + ((a.dim == 3) ? __ldg(T.k2[1] + o) : 0.f);
     mbar_wait(&bar[s], (it >> 1) & 1, a.err);
     ct_fft<NC, false, true, TL>(F, tw, lay);
+#pragma unroll 1
     for (int q = 0; q < a.fanout; ++q) {
       const SpecOp op = a.op[g * a.fanout + q];
+      float2 dconst = make_float2(1.f, 0.f);
+      const float2* dline = nullptr;
+      float e = 0.f;
+      if constexpr (CLS == FC_GRAD) {
+        const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
+        const bool along = (a.dim == 3) ? (op.axis == 2) : (op.axis == 1);
+        if (along)
+          dline = tab;
+        else
+          dconst = __ldg(tab + (op.axis == 0 ? ix : o));
+      } else if constexpr (CLS == FC_NABLA) {
+        e = (op.kind == OP_NABLA1) ? T.ym2 : T.ym1;
+      }
+      // W = F * operator (one pass; positions p = tid + k * (TH / TL))
 #pragma unroll 4
-      for (int i = threadIdx.x; i < E; i += blockDim.x) {
-        const int l = i % TL, p = i / TL;
-        const int ix = min(x0 + l, a.ncols - 1);
-        const int iy = (a.dim == 3) ? o : p;
-        const int iz = (a.dim == 3) ? p : 0;
-        W[i] = c_mul(F[i], eval_op(op, T, a.dim, ix, iy, iz));
+      for (int p = tid; p < NC; p += TH / TL) {
+        const float k = sqrtf(kxy2 + __ldg(kl2 + p));
+        float m;
+        if constexpr (CLS == FC_GRAD) {
+          m = sinc_series(T.cdt2 * k) * T.scale;
+        } else if constexpr (CLS == FC_NABLA) {
+          m = (k == 0.f) ? (e == 0.f ? T.scale : 0.f) : exp2f(e * log2f(k)) * T.scale;
+        } else {
+          m = cos_series(T.cdt2 * k) * T.scale;
+        }
+        float2 f = F[lay(l, p)];
+        f = make_float2(f.x * m, f.y * m);
+        if constexpr (CLS == FC_GRAD) f = c_mul(f, dline ? __ldg(dline + p) : dconst);
+        W[lay(l, p)] = f;
       }
       __syncthreads();
-      ct_fft<NC, true, true, TL>(W, tw, lay);
+      // inverse: stage 0 in place, stage 1 straight to the output buffer
+      ct_stage<NC, 0, true>(W, tw, l, tid, lay);
       float2* dst = a.outp[g * a.fanout + q] + (long long)o * a.ostride + x0;
-#pragma unroll 4
-      for (int i = threadIdx.x; i < E; i += blockDim.x) {
-        const int l = i % TL, p = i / TL;
-        if (x0 + l < a.ncols) dst[p * a.lstride + l] = W[i];
-      }
+      const bool valid = (x0 + l) < a.ncols;
+      auto ld_w = [&](int ll, int pos) -> float2 { return W[lay(ll, pos)]; };
+      auto st_g = [&](int ll, int pos, float2 v) {
+        if (valid) dst[pos * a.lstride + ll] = v;
+      };
+      ct_stage_io<NC, 1, true>(tw, l, tid, ld_w, st_g);
       __syncthreads();
     }
     // F is consumed: refill this input stage with the tile two ahead
@@ -230,10 +266,10 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
   return cudaGetLastError();
 }
 
-template <int NC>
+template <int NC, int CLS>
 static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t);
-  auto k = k_fused_tma<NC>;
+  auto k = k_fused_tma<NC, CLS>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
@@ -241,6 +277,14 @@ static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const Sp
   const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
   k<<<grid, TTile<NC>::THREADS, sm, st>>>(a, tw, T);
   return cudaGetLastError();
+}
+
+template <int NC>
+static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
+  const int kind = a.op[0].kind;
+  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG) return fused_tma_t<NC, FC_GRAD>(a, tw, T, st);
+  if (kind == OP_NABLA1 || kind == OP_NABLA2) return fused_tma_t<NC, FC_NABLA>(a, tw, T, st);
+  return fused_tma_t<NC, FC_SRCK>(a, tw, T, st);
 }
 
 int tma_lines(int n) { return ct_lines_of(n); }
@@ -256,9 +300,9 @@ cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* t
 
 cudaError_t launch_fused_tma(int n, const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   switch (n) {
-    case 64: return fused_tma_t<64>(a, tw, T, st);
-    case 128: return fused_tma_t<128>(a, tw, T, st);
-    case 256: return fused_tma_t<256>(a, tw, T, st);
+    case 64: return fused_tma_cls<64>(a, tw, T, st);
+    case 128: return fused_tma_cls<128>(a, tw, T, st);
+    case 256: return fused_tma_cls<256>(a, tw, T, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -35,12 +35,12 @@ def two_disc_2d(n=128, dx=1e-4, t_end=8e-6, cart_points=50, cart_radius=4e-3):
     return kgrid, medium, source, sensor
 
 
-def het_absorbing_3d(n=256, nt=1200, dx=1e-4, pml=10, plane=48, record=("p_max", "p_rms")):
+def het_absorbing_3d(n=256, nt=1200, dx=1e-4, pml=10, plane=48, record=("p_max", "p_rms"), shape=None):
     """3D heterogeneous, power-law absorbing, nonlinear medium (c = 1500 + 60 z,
     rho = 1000 + 50 z', z smoothed unit-std noise), an additive plane pressure
     source driven by a 1 MHz 3-cycle tone burst of 1 MPa, and every grid
-    point a sensor."""
-    shape = (n, n, n)
+    point a sensor.  `shape` overrides the n^3 grid (profiling cases)."""
+    shape = tuple(shape) if shape else (n, n, n)
     kgrid = KWaveGrid(shape, (dx, dx, dx))
     c = 1500.0 + 60.0 * smoothed_noise(shape, 2)
     rho = 1000.0 + 50.0 * smoothed_noise(shape, 3)
@@ -48,9 +48,9 @@ def het_absorbing_3d(n=256, nt=1200, dx=1e-4, pml=10, plane=48, record=("p_max",
     dt = 0.3 * dx / c.max()
     kgrid.set_time(nt, dt)
     mask = np.zeros(shape)
-    p = min(plane, n - 2 * pml)
-    y0 = (n - p) // 2
-    mask[pml, y0:y0 + p, y0:y0 + p] = 1
+    p = min(plane, min(shape[1:]) - 2 * pml)
+    y0, z0 = (shape[1] - p) // 2, (shape[2] - p) // 2
+    mask[pml, y0:y0 + p, z0:z0 + p] = 1
     sig = 1e6 * tone_burst(1.0 / dt, 1e6, 3)
     source = {"p_mask": mask, "p": sig, "p_mode": "additive"}
     sensor = {"mask": np.ones(shape), "record": list(record)}
