@@ -30,6 +30,13 @@ struct Tile {
   static constexpr int LINES = ct_lines_of(NC);
   static constexpr int THREADS = NC > 0 ? ct_threads_of(NC) : kThreads;
 };
+// Row (x) tiles use half as many lines: smaller blocks, more of them per SM,
+// so their load / transform / store phases overlap.
+template <int NC>
+struct RTile {
+  static constexpr int LINES = NC > 0 ? (ct_lines_of(NC) / 2 > 0 ? ct_lines_of(NC) / 2 : 1) : 0;
+  static constexpr int THREADS = NC > 0 ? (NC / ct_rmax(NC)) * LINES : kThreads;
+};
 
 // Transform the lines of a tile.  Compile-time lengths run in place in `a`;
 // the runtime engine ping-pongs with `b`.  Returns the result buffer.
@@ -58,7 +65,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_col_fft(ColArgs a, const 
   float2* b0 = sm + n;
   float2* b1 = CT ? nullptr : b0 + tl * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
-  float2* g = a.buf[blockIdx.z] + (long long)blockIdx.y * a.ostride;
+  float2* g = a.buf[blockIdx.z] + (long long)(a.outer0 + blockIdx.y) * a.ostride;
   const int c0 = blockIdx.x * tl;
   const int total = tl * n;
 #pragma unroll 4
@@ -120,10 +127,16 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_fused_last(const __grid_c
     __syncthreads();
     float2* R = tile_fft<NC, true, true>(W1, W2, tw, plan, tl, lay);
     float2* dst = a.out[g * a.fanout + o] + off;
+    float2* dst2 = a.dual_out[g * a.fanout + o];
+    const float2 dsc = dst2 ? __ldg(a.dual_tab[g * a.fanout + o] + outer) : make_float2(0.f, 0.f);
+    if (dst2) dst2 += off;
 #pragma unroll 4
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int l = i % tl, p = i / tl, c = c0 + l;
-      if (c < a.ncols) dst[p * a.lstride + c] = R[i];
+      if (c < a.ncols) {
+        dst[p * a.lstride + c] = R[i];
+        if (dst2) dst2[p * a.lstride + c] = c_mul(R[i], dsc);
+      }
     }
     __syncthreads();
   }
@@ -147,7 +160,7 @@ __device__ __forceinline__ void set_comp(float2* b, RowLayout lay, int q, int x,
 // which is the Hermitian projection that real(ifftn(.)) performs.
 template <int NC>
 __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* buf, RowLayout lay, const Dims& d,
-                                         long long r0, int L) {
+                                         long long r0, int L, const float2* __restrict__ kmul = nullptr) {
   if constexpr (NC > 0 && NC % 4 == 0) {
     // paired 16-byte loads; each loaded bin k also fills its mirror n - k
     constexpr int n = NC, np = NC / 4 + 1;  // bin pairs (k, k+1), k even, k <= n/2
@@ -157,8 +170,16 @@ __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* b
       const int l = i / np, k = 2 * (i - l * np);
       const long long ra = r0 + 2 * l, rb = ra + 1;
       float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
-      if (ra < d.nrows) A = *reinterpret_cast<const float4*>(S + ra * d.nxp + k);
-      if (rb < d.nrows) B = *reinterpret_cast<const float4*>(S + rb * d.nxp + k);
+      if (ra < d.row1) A = *reinterpret_cast<const float4*>(S + ra * d.nxp + k);
+      if (rb < d.row1) B = *reinterpret_cast<const float4*>(S + rb * d.nxp + k);
+      if (kmul) {
+        const float2 m0 = __ldg(kmul + k), m1 = __ldg(kmul + min(k + 1, n / 2));
+        float2 t = c_mul(make_float2(A.x, A.y), m0), u = c_mul(make_float2(A.z, A.w), m1);
+        A = make_float4(t.x, t.y, u.x, u.y);
+        t = c_mul(make_float2(B.x, B.y), m0);
+        u = c_mul(make_float2(B.z, B.w), m1);
+        B = make_float4(t.x, t.y, u.x, u.y);
+      }
       if (k == 0) {
         A.y = 0.f;
         B.y = 0.f;
@@ -184,8 +205,13 @@ __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* b
     const long long ra = r0 + 2 * l, rb = ra + 1;
     const int kk = (2 * k <= n) ? k : n - k;
     float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
-    if (ra < d.nrows) A = S[ra * d.nxp + kk];
-    if (rb < d.nrows) B = S[rb * d.nxp + kk];
+    if (ra < d.row1) A = S[ra * d.nxp + kk];
+    if (rb < d.row1) B = S[rb * d.nxp + kk];
+    if (kmul) {
+      const float2 m = __ldg(kmul + kk);
+      A = c_mul(A, m);
+      B = c_mul(B, m);
+    }
     if (2 * k > n) {
       A.y = -A.y;
       B.y = -B.y;
@@ -216,11 +242,11 @@ __device__ __forceinline__ void store_r2c(const float2* buf, float2* __restrict_
       const float4 B = make_float4(0.5f * (z0.y + m0.y), -0.5f * (z0.x - m0.x), 0.5f * (z1.y + m1.y),
                                    -0.5f * (z1.x - m1.x));
       if (k + 1 < nh) {
-        if (ra < d.nrows) *reinterpret_cast<float4*>(S + ra * d.nxp + k) = A;
-        if (rb < d.nrows) *reinterpret_cast<float4*>(S + rb * d.nxp + k) = B;
+        if (ra < d.row1) *reinterpret_cast<float4*>(S + ra * d.nxp + k) = A;
+        if (rb < d.row1) *reinterpret_cast<float4*>(S + rb * d.nxp + k) = B;
       } else {
-        if (ra < d.nrows) S[ra * d.nxp + k] = make_float2(A.x, A.y);
-        if (rb < d.nrows) S[rb * d.nxp + k] = make_float2(B.x, B.y);
+        if (ra < d.row1) S[ra * d.nxp + k] = make_float2(A.x, A.y);
+        if (rb < d.row1) S[rb * d.nxp + k] = make_float2(B.x, B.y);
       }
     }
     return;
@@ -236,8 +262,8 @@ __device__ __forceinline__ void store_r2c(const float2* buf, float2* __restrict_
     const float2 zn = buf[lay(l, k == 0 ? 0 : n - k)];
     const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
     const float2 B = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
-    if (ra < d.nrows) S[ra * d.nxp + k] = A;
-    if (rb < d.nrows) S[rb * d.nxp + k] = B;
+    if (ra < d.row1) S[ra * d.nxp + k] = A;
+    if (rb < d.row1) S[rb * d.nxp + k] = B;
   }
 }
 
@@ -339,7 +365,7 @@ __device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long
 __device__ void sensor_sparse_tile(const Sensor& s, int fi, const float2* buf, RowLayout lay, const Dims& d,
                                    long long r0, int L, int* sh) {
   if (s.mode != 2 || fi <= 0) return;
-  const long long rend = min(r0 + 2LL * L, d.nrows);
+  const long long rend = min(r0 + 2LL * L, d.row1);
   tile_range(s.idx, s.ns, r0 * d.nx, rend * d.nx, sh);
   const int lo = sh[0], hi = sh[1];
   for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
@@ -356,7 +382,7 @@ __device__ __forceinline__ float src_value(const SparseSource& s, const float* s
 
 template <int NC>
 __device__ __forceinline__ int row_lines(int L) {
-  return NC > 0 ? Tile<NC>::LINES : L;
+  return NC > 0 ? RTile<NC>::LINES : L;
 }
 
 // ---------------------------------------------------------------------------
@@ -364,7 +390,7 @@ __device__ __forceinline__ int row_lines(int L) {
 // sources, velocity sensors, R2C of the new velocity.  blockIdx.y = axis.
 // ---------------------------------------------------------------------------
 template <int NC>
-__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
                                                            const __grid_constant__ FFTPlan plan,
                                                            const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
@@ -378,10 +404,10 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
   float2* B0 = sm + nx;
   float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
-  const long long r0 = (long long)blockIdx.x * 2 * L;
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
-  load_c2r<NC>(a.S[ax], B0, lay, d, r0, L);
+  load_c2r<NC>(a.S[ax], B0, lay, d, r0, L, a.kmul[ax]);
   __syncthreads();
   float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
   float2* W = (G == B0) ? B1 : B0;
@@ -399,7 +425,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) {
+      if (row >= d.row1) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) set_comp(G, lay, q, x + j, 0.f);
         continue;
@@ -434,7 +460,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) {
+      if (row >= d.row1) {
         set_comp(G, lay, q, x, 0.f);
         continue;
       }
@@ -458,7 +484,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
   // sparse velocity sources (dirichlet / additive without correction)
   const float* ssig = a.src_sig[ax];
   if (a.src.n > 0 && ssig && t <= a.src_len[ax] && !a.init) {
-    const long long rend = min(r0 + 2LL * L, d.nrows);
+    const long long rend = min(r0 + 2LL * L, d.row1);
     tile_range(a.src.idx, a.src.n, r0 * nx, rend * nx, sh);
     const int lo = sh[0], hi = sh[1];
     for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
@@ -476,7 +502,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) continue;
+      if (row >= d.row1) continue;
       const long long gi = row * nx + x;
       const float4 v = make_float4(get_comp(G, lay, q, x), get_comp(G, lay, q, x + 1), get_comp(G, lay, q, x + 2),
                                    get_comp(G, lay, q, x + 3));
@@ -488,7 +514,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) continue;
+      if (row >= d.row1) continue;
       const long long gi = row * nx + x;
       const float v = get_comp(G, lay, q, x);
       u[gi] = v;
@@ -510,7 +536,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_u(const __grid_constant
 // the local part of p plus the R2C of rho0 * sum(du) and sum(rho).
 // ---------------------------------------------------------------------------
 template <int NC, int DIM>
-__global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
+__global__ void __launch_bounds__(RTile<NC>::THREADS, 4) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
@@ -524,7 +550,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_con
   float2* pool[4];
   for (int b = 0; b < 4; ++b) pool[b] = sm + nx + b * L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
-  const long long r0 = (long long)blockIdx.x * 2 * L;
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
   // inverse x transforms of the divergence components
@@ -572,7 +598,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_con
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) {
+      if (row >= d.row1) {
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           _Pragma("unroll") for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x + j, 0.f);
@@ -655,7 +681,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_con
     if (sp && pass == 1) {
       // apply sparse pressure sources to every rho component in global memory
       __syncthreads();
-      const long long rend = min(r0 + 2LL * L, d.nrows);
+      const long long rend = min(r0 + 2LL * L, d.row1);
       tile_range(a.src.idx, a.src.n, r0 * nx, rend * nx, sh);
       const int lo = sh[0], hi = sh[1];
       for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
@@ -669,7 +695,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_con
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) {
+      if (row >= d.row1) {
         _Pragma("unroll") for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x, 0.f);
         continue;
       }
@@ -749,7 +775,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS, 2) k_x_rho(const __grid_con
 // power-law absorbing EOS: p = p_loc + c0^2 tau A - c0^2 eta B, sensors, R2C.
 // ---------------------------------------------------------------------------
 template <int NC>
-__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_constant__ EosArgs a, Dims d,
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_constant__ EosArgs a, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
@@ -763,7 +789,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_consta
   float2* P1 = P0 + L * lay.ls;
   float2* P2 = CT ? nullptr : P1 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
-  const long long r0 = (long long)blockIdx.x * 2 * L;
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
   const int fi = record_index(a.clk);
   float2 *RA, *RB, *Wk;
   load_c2r<NC>(a.S_a, P0, lay, d, r0, L);
@@ -790,7 +816,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_consta
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) {
+      if (row >= d.row1) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) set_comp(RA, lay, q, x + j, 0.f);
         continue;
@@ -814,7 +840,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_consta
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
-      if (row >= d.nrows) {
+      if (row >= d.row1) {
         set_comp(RA, lay, q, x, 0.f);
         continue;
       }
@@ -838,7 +864,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_eos(const __grid_consta
 // plain x transforms (setup work, sources with k-space correction)
 // ---------------------------------------------------------------------------
 template <int NC>
-__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_r2c(const float* __restrict__ f, float2* S, Dims d,
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_r2c(const float* __restrict__ f, float2* S, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ float2 sm[];
@@ -850,12 +876,12 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_r2c(const float* __rest
   float2* B0 = sm + nx;
   float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
-  const long long r0 = (long long)blockIdx.x * 2 * L;
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
   const int total = 2 * L * nx;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int q = i / nx, x = i - q * nx;
     const long long row = r0 + q;
-    set_comp(B0, lay, q, x, row < d.nrows ? f[row * nx + x] : 0.f);
+    set_comp(B0, lay, q, x, row < d.row1 ? f[row * nx + x] : 0.f);
   }
   __syncthreads();
   float2* F = tile_fft<NC, false, false>(B0, B1, tw, plan, L, lay);
@@ -864,7 +890,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_r2c(const float* __rest
 
 // out = v (accumulate == 0) or out += v
 template <int NC>
-__global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_c2r(const float2* __restrict__ S, float* out,
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_c2r(const float2* __restrict__ S, float* out,
                                                              int accumulate, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
@@ -877,7 +903,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_c2r(const float2* __res
   float2* B0 = sm + nx;
   float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
-  const long long r0 = (long long)blockIdx.x * 2 * L;
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
   load_c2r<NC>(S, B0, lay, d, r0, L);
   __syncthreads();
   float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
@@ -885,7 +911,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_x_c2r(const float2* __res
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int q = i / nx, x = i - q * nx;
     const long long row = r0 + q;
-    if (row >= d.nrows) continue;
+    if (row >= d.row1) continue;
     const long long gi = row * nx + x;
     const float v = get_comp(G, lay, q, x);
     out[gi] = accumulate ? out[gi] + v : v;
@@ -1018,14 +1044,14 @@ cudaError_t launch_fused_last(const FusedArgs& a, int ninputs, long long nouter,
   return cudaGetLastError();
 }
 
-static inline unsigned row_tiles(const Dims& d, int L) { return (unsigned)((d.nrows + 2 * L - 1) / (2 * L)); }
+static inline unsigned row_tiles(const Dims& d, int L) { return (unsigned)((d.row1 - d.row0 + 2 * L - 1) / (2 * L)); }
 
 template <int NC>
 static void x_u_t(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt, cudaStream_t st) {
-  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
   set_smem(k_x_u<NC>, sm);
-  k_x_u<NC><<<dim3(row_tiles(d, L), d.dim), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  k_x_u<NC><<<dim3(row_tiles(d, L), d.dim), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
 }
 
 cudaError_t launch_x_u(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
@@ -1037,14 +1063,14 @@ cudaError_t launch_x_u(const UArgs& a, const Dims& d, const FFTPlan& plan, const
 template <int NC>
 static void x_rho_t(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
                     cudaStream_t st) {
-  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? d.dim : d.dim + 1);
   if (d.dim == 3) {
     set_smem(k_x_rho<NC, 3>, sm);
-    k_x_rho<NC, 3><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+    k_x_rho<NC, 3><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
   } else {
     set_smem(k_x_rho<NC, 2>, sm);
-    k_x_rho<NC, 2><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+    k_x_rho<NC, 2><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
   }
 }
 
@@ -1057,10 +1083,10 @@ cudaError_t launch_x_rho(const RhoArgs& a, const Dims& d, const FFTPlan& plan, c
 template <int NC>
 static void x_eos_t(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
                     cudaStream_t st) {
-  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 2 : 3);
   set_smem(k_x_eos<NC>, sm);
-  k_x_eos<NC><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  k_x_eos<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
 }
 
 cudaError_t launch_x_eos(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
@@ -1072,10 +1098,10 @@ cudaError_t launch_x_eos(const EosArgs& a, const Dims& d, const FFTPlan& plan, c
 template <int NC>
 static void x_r2c_t(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
                     cudaStream_t st) {
-  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
   set_smem(k_x_r2c<NC>, sm);
-  k_x_r2c<NC><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(f, S, d, plan, tw, L);
+  k_x_r2c<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(f, S, d, plan, tw, L);
 }
 
 cudaError_t launch_x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
@@ -1087,10 +1113,10 @@ cudaError_t launch_x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan
 template <int NC>
 static void x_c2r_t(const float2* S, float* out, int acc, const Dims& d, const FFTPlan& plan, const float2* tw,
                     int Lrt, cudaStream_t st) {
-  const int L = NC > 0 ? Tile<NC>::LINES : Lrt;
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
   set_smem(k_x_c2r<NC>, sm);
-  k_x_c2r<NC><<<row_tiles(d, L), Tile<NC>::THREADS, sm, st>>>(S, out, acc, d, plan, tw, L);
+  k_x_c2r<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(S, out, acc, d, plan, tw, L);
 }
 
 cudaError_t launch_x_c2r(const float2* S, float* out, int accumulate, const Dims& d, const FFTPlan& plan,

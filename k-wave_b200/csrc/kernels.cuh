@@ -19,6 +19,7 @@ struct Dims {
   int nxp;          // spectral row pitch (complex elements)
   long long nrows;  // ny * nz
   long long npts;   // nx * ny * nz
+  long long row0, row1;  // rows [row0, row1) processed by a row-kernel launch
 };
 
 enum SpecOpKind {
@@ -28,6 +29,7 @@ enum SpecOpKind {
   OP_NABLA2 = 3,     // |k|^(y-1)
   OP_SRC_KAPPA = 4,  // cos(c_ref |k| dt / 2)
   OP_IDENTITY = 5,
+  OP_KAPPA = 6,      // kappa alone (the axis factor applied elsewhere)
 };
 
 struct SpecOp {
@@ -100,6 +102,7 @@ struct Sensor {
 // ---------------------------------------------------------------------------
 struct ColArgs {
   float2* buf[4];     // fields transformed in place (blockIdx.z)
+  int outer0;         // first outer index (z plane) of this launch
   int ncols;          // valid columns (kx values)
   long long lstride;  // element stride along the transformed axis
   long long ostride;  // stride of the outer index (blockIdx.y)
@@ -110,6 +113,8 @@ struct FusedArgs {
   const float2* in[3];  // inputs (blockIdx.z)
   float2* out[9];       // outputs [input * fanout + o]
   SpecOp op[9];
+  float2* dual_out[9];         // optional second output: out times dual_tab[outer]
+  const float2* dual_tab[9];
   int fanout;
   int ncols;
   long long lstride, ostride;
@@ -118,6 +123,7 @@ struct FusedArgs {
 
 struct UArgs {
   const float2* S[3];  // gradient spectra, already inverse-transformed along y / z
+  const float2* kmul[3];  // optional kx multiplier applied as the spectra are read
   float2* Sout[3];     // receives the x-transform of the new velocity
   float* u[3];
   Map rinv[3];         // 1 / rho0 on the staggered grids

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
     f = t / per_field;
     const int r = t - f * per_field;
     const int o = r / a.ncx;
-    tile_coords(a.yaxis, r - o * a.ncx, o, TL, x, y, z);
+    tile_coords(a.yaxis, r - o * a.ncx, a.outer0 + o, TL, x, y, z);
   };
   auto issue = [&](int t, int s) {
     int f, x, y, z;
@@ -163,12 +163,14 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
       const float2* dline = nullptr;
       float e = 0.f;
       if constexpr (CLS == FC_GRAD) {
-        const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
-        const bool along = (a.dim == 3) ? (op.axis == 2) : (op.axis == 1);
-        if (along)
-          dline = tab;
-        else
-          dconst = __ldg(tab + (op.axis == 0 ? ix : o));
+        if (op.kind != OP_KAPPA) {
+          const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
+          const bool along = (a.dim == 3) ? (op.axis == 2) : (op.axis == 1);
+          if (along)
+            dline = tab;
+          else
+            dconst = __ldg(tab + (op.axis == 0 ? ix : o));
+        }
       } else if constexpr (CLS == FC_NABLA) {
         e = (op.kind == OP_NABLA1) ? T.ym2 : T.ym1;
       }
@@ -193,10 +195,20 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
       // inverse: stage 0 in place, stage 1 straight to the output buffer
       ct_stage<NC, 0, true>(W, tw, l, tid, lay);
       float2* dst = a.outp[g * a.fanout + q] + (long long)o * a.ostride + x0;
+      // optional second output scaled by a factor constant along the line
+      float2* dst2 = a.dual_outp[g * a.fanout + q];
+      float2 dsc = make_float2(0.f, 0.f);
+      if (dst2) {
+        dst2 += (long long)o * a.ostride + x0;
+        dsc = __ldg(a.dual_tab[g * a.fanout + q] + o);
+      }
       const bool valid = (x0 + l) < a.ncols;
       auto ld_w = [&](int ll, int pos) -> float2 { return W[lay(ll, pos)]; };
       auto st_g = [&](int ll, int pos, float2 v) {
-        if (valid) dst[pos * a.lstride + ll] = v;
+        if (valid) {
+          dst[pos * a.lstride + ll] = v;
+          if (dst2) dst2[pos * a.lstride + ll] = c_mul(v, dsc);
+        }
       };
       ct_stage_io<NC, 1, true>(tw, l, tid, ld_w, st_g);
       __syncthreads();
@@ -282,7 +294,7 @@ static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const Sp
 template <int NC>
 static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   const int kind = a.op[0].kind;
-  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG) return fused_tma_t<NC, FC_GRAD>(a, tw, T, st);
+  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA) return fused_tma_t<NC, FC_GRAD>(a, tw, T, st);
   if (kind == OP_NABLA1 || kind == OP_NABLA2) return fused_tma_t<NC, FC_NABLA>(a, tw, T, st);
   return fused_tma_t<NC, FC_SRCK>(a, tw, T, st);
 }

@@ -10,7 +10,8 @@ struct ColTmaArgs {
   CUtensorMap map[4];  // one per field; box {LINES, N, 1} (y pass) or {LINES, 1, N} (last axis)
   int nfields;
   int ncx;      // column tiles along kx
-  int nouter;   // outer extent (z for the y pass, y for the 3D last axis)
+  int nouter;   // outer extent of this launch (z planes for the y pass)
+  int outer0;   // first outer index
   int yaxis;    // 1: the transformed axis is the tensor's y dimension, 2: z
   int* err;
 };
@@ -20,6 +21,8 @@ struct FusedTmaArgs {
   CUtensorMap out[9];
   SpecOp op[9];
   float2* outp[9];      // output buffers (written with plain stores)
+  float2* dual_outp[9];         // optional second output: outp times dual_tab[outer]
+  const float2* dual_tab[9];
   long long lstride;    // element stride along the transformed axis
   long long ostride;    // stride of the outer index
   int nin, fanout, ncx, nouter, yaxis, dim;

@@ -201,6 +201,8 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   d.nxp = (d.nxh + 31) / 32 * 32;  // whole TMA column tiles: no box leaves the buffer
   d.nrows = (long long)d.ny * d.nz;
   d.npts = (long long)d.nx * d.nrows;
+  d.row0 = 0;
+  d.row1 = d.nrows;
   if (d.npts >= (1LL << 31)) throw KwError(KW_ERR_UNSUPPORTED, "grids above 2^31 points are not supported");
   Nt = in->Nt;
   if (!(in->dx > 0) || !(in->dy > 0) || (d.dim == 3 && !(in->dz > 0)) || !(in->dt > 0))
@@ -344,6 +346,8 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   }
   err_buf.alloc(sizeof(int));
   ck(cudaMemsetAsync(err_buf.p, 0, sizeof(int), st), "memset");
+  const char* no_graph = std::getenv("KWAVE_B200_NO_GRAPH");
+  use_graph = !(no_graph && no_graph[0] == '1');
   // TMA-fed column passes for the compile-time lengths they support
   const char* no_tma = std::getenv("KWAVE_B200_NO_TMA");
   const bool tma_ok = !(no_tma && no_tma[0] == '1');
@@ -352,6 +356,18 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   for (int s = 0; s < 4; ++s) {
     if (use_tma[1] && !make_spec_map(&map_y[s], S_buf[s].p, d, 1, d.ny)) use_tma[1] = false;
     if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;
+  }
+  // z slabs of the y-inverse / row kernel / y-forward chains.  Measured on
+  // 256^3: whole-volume launches (one slab) are fastest -- the per-slab
+  // launches lose more to partial waves than L2 reuse of the slab's half
+  // spectra gains -- so one slab is the default; KWAVE_B200_SLAB sets the
+  // planes per slab.
+  {
+    int zs = d.nz;
+    const char* env = std::getenv("KWAVE_B200_SLAB");
+    if (env && std::atoi(env) > 0) zs = std::min(std::atoi(env), d.nz);
+    const int nslab = (d.nz + zs - 1) / zs;
+    slab = (d.nz + nslab - 1) / nslab;
   }
   if (eos == 1) ploc_buf.alloc(fb);
   if (opt.p_final) {
@@ -491,37 +507,44 @@ void Session::corrected_source(float* out, const int* idx, const int* slot, int 
   ck(launch_x_c2r(S, out, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
 }
 
-// y passes (3D) around the fused last-axis operator.  `ins` / `outs` index
-// the half-spectrum work buffers, which hold x-transformed data on entry
-// and on exit (ready for the row kernels).
-void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout) {
+// The y pass (3D) over z planes [z0, z0 + nzs) of the listed half-spectrum
+// buffers, forward or inverse.
+void Session::col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs) {
+  if (d.dim != 3 || bufs.empty()) return;
+  const int n = (int)bufs.size();
+  if (use_tma[1]) {
+    ColTmaArgs ca;
+    std::memset(&ca, 0, sizeof(ca));
+    for (int i = 0; i < n; ++i) ca.map[i] = map_y[bufs[i]];
+    ca.nfields = n;
+    ca.ncx = (d.nxh + tma_lines(d.ny) - 1) / tma_lines(d.ny);
+    ca.nouter = nzs;
+    ca.outer0 = z0;
+    ca.yaxis = 1;
+    ca.err = (int*)err_buf.p;
+    ck(launch_col_tma(inv, d.ny, ca, twd[1], st), "col_tma");
+  } else {
+    ColArgs ca{};
+    for (int i = 0; i < n; ++i) ca.buf[i] = (float2*)S_buf[bufs[i]].p;
+    ca.outer0 = z0;
+    ca.ncols = d.nxh;
+    ca.lstride = d.nxp;
+    ca.ostride = (long long)d.nxp * d.ny;
+    ca.tl = col_tl[1];
+    ck(launch_col_fft(inv, ca, n, nzs, plan[1], twd[1], st), "col_fft");
+  }
+  ++launches_;
+}
+
+// The last-axis operator (z in 3D, y in 2D) over the whole volume: forward
+// transform, multiply by `fanout` operators per input, inverse transforms.
+void Session::fused_pass(const std::vector<int>& ins, const std::vector<int>& outs, const std::vector<SpecOp>& ops,
+                         int fanout, const std::vector<int>& dual, const float2* dual_tab) {
   const int nin = (int)ins.size();
   const int nout = (int)outs.size();
   const int last = d.dim - 1;
   const int ns[3] = {d.nx, d.ny, d.nz};
   auto Sp = [&](int i) { return (float2*)S_buf[i].p; };
-  if (d.dim == 3) {
-    if (use_tma[1]) {
-      ColTmaArgs ca;
-      std::memset(&ca, 0, sizeof(ca));
-      for (int i = 0; i < nin; ++i) ca.map[i] = map_y[ins[i]];
-      ca.nfields = nin;
-      ca.ncx = (d.nxh + tma_lines(d.ny) - 1) / tma_lines(d.ny);
-      ca.nouter = d.nz;
-      ca.yaxis = 1;
-      ca.err = (int*)err_buf.p;
-      ck(launch_col_tma(false, d.ny, ca, twd[1], st), "col_tma fwd");
-    } else {
-      ColArgs ca{};
-      for (int i = 0; i < nin; ++i) ca.buf[i] = Sp(ins[i]);
-      ca.ncols = d.nxh;
-      ca.lstride = d.nxp;
-      ca.ostride = (long long)d.nxp * d.ny;
-      ca.tl = col_tl[1];
-      ck(launch_col_fft(false, ca, nin, d.nz, plan[1], twd[1], st), "col_fft fwd");
-    }
-    ++launches_;
-  }
   if (use_tma[last]) {
     FusedTmaArgs fa;
     std::memset(&fa, 0, sizeof(fa));
@@ -531,6 +554,10 @@ void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vec
       fa.out[i] = maps[outs[i]];
       fa.outp[i] = Sp(outs[i]);
       fa.op[i] = ops[i];
+      if (i < (int)dual.size() && dual[i] >= 0) {
+        fa.dual_outp[i] = Sp(dual[i]);
+        fa.dual_tab[i] = dual_tab;
+      }
     }
     fa.lstride = (long long)d.nxp * (d.dim == 3 ? d.ny : 1);
     fa.ostride = d.nxp;
@@ -549,6 +576,10 @@ void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vec
     for (int i = 0; i < nout; ++i) {
       fa.out[i] = Sp(outs[i]);
       fa.op[i] = ops[i];
+      if (i < (int)dual.size() && dual[i] >= 0) {
+        fa.dual_out[i] = Sp(dual[i]);
+        fa.dual_tab[i] = dual_tab;
+      }
     }
     fa.fanout = fanout;
     fa.ncols = d.nxh;
@@ -558,28 +589,35 @@ void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vec
     ck(launch_fused_last(fa, nin, d.dim == 3 ? d.ny : 1, plan[last], twd[last], T, d.dim, st), "fused_last");
   }
   ++launches_;
-  if (d.dim == 3) {
-    if (use_tma[1]) {
-      ColTmaArgs ca;
-      std::memset(&ca, 0, sizeof(ca));
-      for (int i = 0; i < nout; ++i) ca.map[i] = map_y[outs[i]];
-      ca.nfields = nout;
-      ca.ncx = (d.nxh + tma_lines(d.ny) - 1) / tma_lines(d.ny);
-      ca.nouter = d.nz;
-      ca.yaxis = 1;
-      ca.err = (int*)err_buf.p;
-      ck(launch_col_tma(true, d.ny, ca, twd[1], st), "col_tma inv");
-    } else {
-      ColArgs ca{};
-      for (int i = 0; i < nout; ++i) ca.buf[i] = Sp(outs[i]);
-      ca.ncols = d.nxh;
-      ca.lstride = d.nxp;
-      ca.ostride = (long long)d.nxp * d.ny;
-      ca.tl = col_tl[1];
-      ck(launch_col_fft(true, ca, nout, d.nz, plan[1], twd[1], st), "col_fft inv");
-    }
-    ++launches_;
-  }
+}
+
+// A whole-volume spectral operation on x-transformed buffers: y forward,
+// last-axis operator, y inverse (setup work and "many"-signal sources).
+void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout) {
+  col_pass(false, ins, 0, d.nz);
+  fused_pass(ins, outs, ops, fanout);
+  col_pass(true, outs, 0, d.nz);
+}
+
+// Gradient of p along each axis (kspaceFirstOrder3D.m:790-801) from S0
+// (transformed along x and y) into S1..S3, still transformed along x and y.
+// The x and y derivative factors do not vary along the last axis, so one
+// inverse transform of kappa * F{p} serves both: S1 = F_z^-1{kappa F_z S0}
+// (the x factor is applied when the row kernel reads S1), S2 = ddy(ky) S1,
+// S3 = F_z^-1{ddz kappa F_z S0}.  In 2D the last axis is y: S1 as above,
+// S2 = F_y^-1{ddy kappa F_y S0}.
+void Session::grad_pass() {
+  if (d.dim == 3)
+    fused_pass({0}, {1, 3}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 2}}, 2, {2, -1}, T.ddk_pos[1]);
+  else
+    fused_pass({0}, {1, 2}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 1}}, 2);
+}
+
+Dims Session::slab_dims(int z0, int nzs) const {
+  Dims s = d;
+  s.row0 = (long long)z0 * d.ny;
+  s.row1 = (long long)(z0 + nzs) * d.ny;
+  return s;
 }
 
 void Session::setup_sensors(const kw_input* in) {
@@ -702,26 +740,27 @@ void Session::enqueue_init() {
   float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
   ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
   ++launches_;
+  col_pass(false, {0}, 0, d.nz);
+  grad_pass();
   std::vector<int> outs;
-  std::vector<SpecOp> ops;
-  for (int a = 0; a < d.dim; ++a) {
-    outs.push_back(a + 1);
-    ops.push_back(SpecOp{OP_GRAD_POS, a});
-  }
-  run_spectral({0}, outs, ops, d.dim);
+  for (int a = 0; a < d.dim; ++a) outs.push_back(a + 1);
+  col_pass(true, outs, 0, d.nz);
   UArgs ua = u_args(S);
   ua.init = 1;
   ua.do_r2c = 0;
   ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u init");
   ++launches_;
+  // the x and y transforms of p for the next step's gradient
   ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
   ++launches_;
+  col_pass(false, {0}, 0, d.nz);
   if (p_buf.p)
     ck(cudaMemcpyAsync(p_buf.p, p0d, sizeof(float) * d.npts, cudaMemcpyDeviceToDevice, st), "p0 copy");
 }
 
 UArgs Session::u_args(float2* const* S) {
   UArgs ua{};
+  ua.kmul[0] = T.ddk_pos[0];  // the x derivative factor, applied as S1 is read
   for (int a = 0; a < d.dim; ++a) {
     ua.S[a] = S[a + 1];
     ua.Sout[a] = S[a + 1];
@@ -741,40 +780,80 @@ UArgs Session::u_args(float2* const* S) {
   return ua;
 }
 
+// One time step (kspaceFirstOrder3D.m:767-1206) as three chains, each a
+// whole-volume last-axis operator followed, per z slab, by the y inverse,
+// the fused row kernel and the y forward transform of its outputs.  A slab's
+// half spectra stay in L2 from one kernel of the chain to the next.
+// On entry S0 holds p transformed along x and y; on exit too.
+// Steps whose launch sequence is the same every time (no initial-pressure
+// start, not the last step, no per-step "many"-signal corrected source) are
+// captured once as a CUDA graph and replayed: every time-dependent value
+// (record index, source sample) is read on the device from the clock.
+bool Session::graphable(uint64_t t) const {
+  if (!use_graph) return false;
+  if (t == 1 && p0) return false;
+  if (t == Nt) return false;
+  for (int a = 0; a < d.dim; ++a)
+    if (u_many_additive && udense[a].field && (int)t <= u_len[a]) return false;
+  if (p_many_additive && (int)t <= p_len) return false;
+  return true;
+}
+
 void Session::enqueue_step() {
   const uint64_t t = t_done + 1;
+  if (graphable(t)) {
+    if (!graph_exec) {
+      cudaGraph_t g = nullptr;
+      ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+      const uint64_t l0 = launches_;
+      enqueue_step_body(t);
+      graph_launches = launches_ - l0;
+      launches_ = l0;
+      ck(cudaStreamEndCapture(st, &g), "end capture");
+      graph = g;
+      ck(cudaGraphInstantiate(&graph_exec, graph, 0), "graph instantiate");
+    }
+    ck(cudaGraphLaunch(graph_exec, st), "graph launch");
+    launches_ += graph_launches;
+  } else {
+    enqueue_step_body(t);
+  }
+  ++t_done;
+}
+
+void Session::enqueue_step_body(uint64_t t) {
   if (t == 1 && p0) {
     enqueue_init();
   } else {
     float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
+    std::vector<int> f123, f12;
+    for (int a = 0; a < d.dim; ++a) f123.push_back(a + 1);
+    f12 = {1, 2};
+    const bool last = (t == Nt);
     // (1) momentum: grad p -> u (kspaceFirstOrder3D.m:790-884)
-    std::vector<int> outs;
-    std::vector<SpecOp> ops;
-    for (int a = 0; a < d.dim; ++a) {
-      outs.push_back(a + 1);
-      ops.push_back(SpecOp{OP_GRAD_POS, a});
-    }
-    run_spectral({0}, outs, ops, d.dim);
+    grad_pass();
     if (u_many_additive) {
       for (int a = 0; a < d.dim; ++a)
         if (udense[a].field && (int)t <= u_len[a]) {
-          // S[0] is free here: the gradient has been taken
+          // S0 is free here: the gradient has been taken
           corrected_source_into((float*)ufield_buf[a].p, (const int*)usrc_idx.p, (const int*)usrc_slot.p, u_nsrc,
                                 usig_d[a], u_nsig, (int)t, 0);
         }
     }
     UArgs ua = u_args(S);
-    ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u");
-    ++launches_;
-    // (2) mass conservation: div u -> rho, EOS (:905-1017)
-    std::vector<int> ins2, outs2;
-    std::vector<SpecOp> ops2;
-    for (int a = 0; a < d.dim; ++a) {
-      ins2.push_back(a + 1);
-      outs2.push_back(a + 1);
-      ops2.push_back(SpecOp{OP_GRAD_NEG, a});
+    for (int z0 = 0; z0 < d.nz; z0 += slab) {
+      const int nzs = std::min(slab, d.nz - z0);
+      col_pass(true, f123, z0, nzs);
+      ck(launch_x_u(ua, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_u");
+      ++launches_;
+      col_pass(false, f123, z0, nzs);
     }
-    run_spectral(ins2, outs2, ops2, 1);
+    // (2) mass conservation: div u -> rho, EOS (:905-1017)
+    {
+      std::vector<SpecOp> ops;
+      for (int a = 0; a < d.dim; ++a) ops.push_back(SpecOp{OP_GRAD_NEG, a});
+      fused_pass(f123, f123, ops, 1);
+    }
     if (p_many_additive && (int)t <= p_len)
       corrected_source_into((float*)psrc_field.p, (const int*)psrc_idx.p, (const int*)psrc_slot.p, p_nsrc,
                             (const float*)psrc_sig.p, p_nsig, (int)t, 0);
@@ -795,7 +874,6 @@ void Session::enqueue_step() {
     ra.dsrc = pdense;
     ra.sens = sens_p;
     ra.clk = clk;
-    const bool last = (t == Nt);
     if (eos == 1) {
       ra.p_loc = (float*)ploc_buf.p;
       ra.S_q = S[1];
@@ -804,11 +882,19 @@ void Session::enqueue_step() {
       ra.p_out = last ? (float*)p_buf.p : nullptr;
       ra.S_p = S[0];
     }
-    ck(launch_x_rho(ra, d, plan[0], twd[0], rowL, st), "x_rho");
-    ++launches_;
+    for (int z0 = 0; z0 < d.nz; z0 += slab) {
+      const int nzs = std::min(slab, d.nz - z0);
+      col_pass(true, f123, z0, nzs);
+      ck(launch_x_rho(ra, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_rho");
+      ++launches_;
+      if (eos == 1)
+        col_pass(false, f12, z0, nzs);
+      else
+        col_pass(false, {0}, z0, nzs);
+    }
     if (eos == 1) {
       // (3) power-law absorption and dispersion (:970-977)
-      run_spectral({1, 2}, {1, 2}, {SpecOp{OP_NABLA1, 0}, SpecOp{OP_NABLA2, 0}}, 1);
+      fused_pass(f12, f12, {SpecOp{OP_NABLA1, 0}, SpecOp{OP_NABLA2, 0}}, 1);
       EosArgs ea{};
       ea.S_a = S[1];
       ea.S_b = S[2];
@@ -819,13 +905,17 @@ void Session::enqueue_step() {
       ea.S_p = S[0];
       ea.sens = sens_p;
       ea.clk = clk;
-      ck(launch_x_eos(ea, d, plan[0], twd[0], rowL, st), "x_eos");
-      ++launches_;
+      for (int z0 = 0; z0 < d.nz; z0 += slab) {
+        const int nzs = std::min(slab, d.nz - z0);
+        col_pass(true, f12, z0, nzs);
+        ck(launch_x_eos(ea, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_eos");
+        ++launches_;
+        col_pass(false, {0}, z0, nzs);
+      }
     }
   }
   ck(launch_advance((int*)clock_buf.p, st), "advance");
   ++launches_;
-  ++t_done;
 }
 
 // corrected source field for "many" signals, using `work` as spectral scratch
@@ -904,6 +994,8 @@ void Session::read(kw_output* out) {
 
 Session::~Session() {
   if (st) cudaStreamSynchronize(st);
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (st) cudaStreamDestroy(st);

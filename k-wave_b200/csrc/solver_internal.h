@@ -54,8 +54,15 @@ class Session {
   void corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
                              int nrows_sig, int t, int work_i);
   void run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout);
+  void col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs);
+  void fused_pass(const std::vector<int>& ins, const std::vector<int>& outs, const std::vector<SpecOp>& ops,
+                  int fanout, const std::vector<int>& dual = {}, const float2* dual_tab = nullptr);
+  void grad_pass();
+  Dims slab_dims(int z0, int nzs) const;
   void enqueue_init();
   void enqueue_step();
+  void enqueue_step_body(uint64_t t);
+  bool graphable(uint64_t t) const;
   UArgs u_args(float2* const* S);
 
   kw_options opt{};
@@ -64,6 +71,12 @@ class Session {
   const float2* twd[3]{};
   int col_tl[3]{16, 16, 16};
   int rowL = 8;
+  int slab = 1;  // z planes per chain slab
+  // captured steady-state step
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  uint64_t graph_launches = 0;
   SpecTables T{};
   float dtf = 0.f;
   bool nonlinear = false;

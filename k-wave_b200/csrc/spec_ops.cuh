@@ -70,6 +70,8 @@ __device__ __forceinline__ float2 eval_op(const SpecOp& op, const SpecTables& T,
         v = exp2f(e * log2f(k));
       return make_float2(v * T.scale, 0.f);
     }
+    case OP_KAPPA:
+      return make_float2(sinc_series(T.cdt2 * k) * T.scale, 0.f);
     case OP_SRC_KAPPA:
       return make_float2(cos_series(T.cdt2 * k) * T.scale, 0.f);
     default:
