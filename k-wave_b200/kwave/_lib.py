@@ -245,7 +245,7 @@ def make_input(inp: dict):
         s.sensor_mask_index = _uptr(idx)
         s.sensor_mask_index_numel = idx.size
     else:
-        cor = keep.u64(np.asarray(inp["sensor_mask_corners"]).reshape(6, -1))
+        cor = keep.u64(inp["sensor_mask_corners"])  # (6, K) column-major: one cuboid per 6 values
         s.sensor_mask_corners = _uptr(cor)
         s.sensor_mask_corners_numel = cor.size
     return s, keep

@@ -1,0 +1,143 @@
+"""Pin the CPU oracle to the reference's own self-consistency tests.
+
+The reference ships no golden vectors, so the oracle is checked against the
+identities its unit tests assert (k-Wave/testing/unit/):
+  * kspaceFirstOrder3D_p0_vs_two_clicks.m: an initial pressure equals two
+    additive-no-correction source clicks of [0.5, 0.5] / (2 c dt / dx);
+  * kspaceFirstOrder3D_compare_binary_and_cuboid_sensor_mask.m;
+  * kspaceFirstOrder2D_compare_labelled_and_binary_source_mask.m;
+  * kspaceFirstOrder_compare_1D_2D_3D_plane_waves.m (axis symmetry);
+and the FP32 restatement is checked against the FP64 one (DataCast 'off').
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+from kwave.simulation import prepare
+from kwave.utils import KWaveGrid, make_ball, make_disc
+from oracle.kspace_oracle import simulate
+
+
+def _pair(dim):
+    if dim == 3:
+        n = (32, 32, 32)
+        p0 = make_ball(*n, 16, 16, 16, 6)
+        mask = np.zeros(n)
+        mask[[3, 28], :, :] = 1
+    else:
+        n = (64, 64)
+        p0 = make_disc(*n, 32, 32, 10)
+        mask = np.zeros(n)
+        mask[[5, 58], :] = 1
+    kg = KWaveGrid(n, (1e-4,) * dim)
+    kg.make_time(1500.0, 0.234)
+    kg.set_time(min(kg.Nt, 60), kg.dt)
+    medium = {"sound_speed": 1500.0, "density": 1000.0}
+    sensor = {"mask": mask, "record": ["p"]}
+    a, rec, _, _ = prepare(kg, medium, {"p0": p0}, sensor, smooth_p0=False, pml_alpha=0.0)
+    src = {"p_mask": (p0 != 0).astype(float), "p_mode": "additive-no-correction",
+           "p": np.array([[0.5, 0.5]]) / (2 * 1500.0 * kg.dt / kg.dx)}
+    b, _, _, _ = prepare(kg, medium, src, sensor, smooth_p0=False, pml_alpha=0.0)
+    return a, b, rec
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_p0_equals_two_clicks(dim):
+    a, b, rec = _pair(dim)
+    pa = simulate(a, rec, dtype=np.float64)["p"]
+    pb = simulate(b, rec, dtype=np.float64)["p"]
+    if dim == 3:
+        # the reference's criterion: max(sensor_data(:) - sensor_data2(:)) <= 1e-14
+        assert np.max(pa - pb) <= 1e-14
+    # both directions, relative to the signal
+    assert np.max(np.abs(pa - pb)) <= 1e-12 * np.max(np.abs(pa))
+
+
+def test_cuboid_equals_binary_mask():
+    n = (24, 26, 28)
+    kg = KWaveGrid(n, (1e-4,) * 3)
+    kg.set_time(30, 0.3e-4 / 1500)
+    p0 = make_ball(*n, 12, 13, 14, 3)
+    corners = np.array([[3, 4, 5, 9, 10, 8], [15, 14, 20, 20, 19, 25]]).T
+    rec = ["p", "p_max", "p_rms", "u", "u_max"]
+    medium = {"sound_speed": 1500.0, "density": 1000.0}
+    ic, record, _, _ = prepare(kg, medium, {"p0": p0}, {"mask": corners, "record": rec}, pml_size=4)
+    ib = dict(ic)
+    ib.pop("sensor_mask_corners")
+    ib["sensor_mask_type"] = 0
+    lin = []
+    for k in range(corners.shape[1]):
+        x1, y1, z1, x2, y2, z2 = corners[:, k]
+        sub = np.zeros(n, dtype=bool)
+        sub[x1 - 1:x2, y1 - 1:y2, z1 - 1:z2] = True
+        lin.append(np.flatnonzero(sub.reshape(-1, order="F")) + 1)
+    ib["sensor_mask_index"] = np.concatenate(lin)
+    oc = simulate(ic, record, dtype=np.float64)
+    ob = simulate(ib, record, dtype=np.float64)
+    for k in ob:
+        np.testing.assert_array_equal(oc[k], ob[k])
+
+
+def test_labelled_equals_binary_source():
+    n = (48, 40)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    kg.set_time(60, 0.3e-4 / 1500)
+    lab = np.zeros(n)
+    lab[10, 5:15] = 1
+    lab[30, 20:32] = 2
+    lab[20:26, 35] = 3
+    t = np.arange(kg.Nt) * kg.dt
+    sig = np.vstack([0.5 * np.sin(2 * np.pi * 1e6 * t), 0.8 * np.sin(2 * np.pi * 2e6 * t),
+                     0.2 * np.sin(2 * np.pi * 0.5e6 * t)])
+    medium = {"sound_speed": 1500.0, "density": 1000.0}
+    sensor = {"mask": np.ones(n), "record": ["p_final", "p_max"]}
+    il, rec, _, _ = prepare(kg, medium, {"p_mask": lab, "p": sig}, sensor, pml_size=6)
+    index_mask = lab.reshape(-1, order="F")[lab.reshape(-1, order="F") != 0].astype(int)
+    ib, _, _, _ = prepare(kg, medium, {"p_mask": (lab != 0).astype(float), "p": sig[index_mask - 1]}, sensor,
+                          pml_size=6)
+    ol = simulate(il, rec, dtype=np.float64)
+    ob = simulate(ib, rec, dtype=np.float64)
+    for k in ("p_final", "p_max"):
+        assert np.max(np.abs(ol[k] - ob[k])) <= 1e-15 * np.max(np.abs(ob[k])) + 1e-300
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_plane_wave_axis_symmetry(dim):
+    """A plane wave launched along each axis gives the same (transposed) field."""
+    n = 32
+    shape = (n,) * dim
+    kg = KWaveGrid(shape, (1e-4,) * dim)
+    kg.set_time(40, 0.3e-4 / 1500)
+    t = np.arange(kg.Nt) * kg.dt
+    sig = np.sin(2 * np.pi * 1.5e6 * t)[None, :] * (t[None, :] < 2e-6)
+    medium = {"sound_speed": 1500.0, "density": 1000.0}
+    finals = []
+    for axis in range(dim):
+        mask = np.zeros(shape)
+        sl = [slice(None)] * dim
+        sl[axis] = 4
+        mask[tuple(sl)] = 1
+        inp, rec, _, _ = prepare(kg, medium, {"p_mask": mask, "p": sig},
+                                 {"mask": np.ones(shape), "record": ["p_final"]}, pml_size=0)
+        pf = simulate(inp, rec, dtype=np.float64)["p_final"]
+        finals.append(np.moveaxis(pf, axis, 0))
+    for f in finals[1:]:
+        assert np.max(np.abs(f - finals[0])) <= 1e-12 * np.max(np.abs(finals[0]))
+
+
+def test_fp32_restatement_tracks_fp64():
+    n = (40, 36, 30)
+    rng = np.random.default_rng(3)
+    kg = KWaveGrid(n, (1e-4,) * 3)
+    c = 1500 + 40 * rng.standard_normal(n)
+    kg.set_time(40, 0.3e-4 / c.max())
+    medium = {"sound_speed": c, "density": 1000 + 30 * rng.standard_normal(n), "alpha_coeff": 0.75,
+              "alpha_power": 1.5, "BonA": 6.0}
+    p0 = 1e5 * make_ball(*n, 20, 18, 15, 4)
+    mask = np.zeros(n)
+    mask[::4, ::5, ::3] = 1
+    inp, rec, _, _ = prepare(kg, medium, {"p0": p0}, {"mask": mask, "record": ["p", "p_rms", "u"]}, pml_size=5)
+    o64 = simulate(inp, rec, dtype=np.float64)
+    o32 = simulate(inp, rec, dtype=np.float32)
+    for k in o64:
+        assert rel_l2(o32[k], o64[k]) < 1e-5, k
