@@ -18,7 +18,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("KWAVE_B200_LIB", os.path.join(os.path.dirname(_HERE), "libkwave_b200.so"))
 
-KW_OK = 0
+(KW_OK, KW_ERR_INVALID_ARGUMENT, KW_ERR_CUDA, KW_ERR_OUT_OF_MEMORY, KW_ERR_IO, KW_ERR_UNSUPPORTED,
+ KW_ERR_INTERNAL) = range(7)
 STATUS_NAMES = {0: "KW_OK", 1: "KW_ERR_INVALID_ARGUMENT", 2: "KW_ERR_CUDA", 3: "KW_ERR_OUT_OF_MEMORY",
                 4: "KW_ERR_IO", 5: "KW_ERR_UNSUPPORTED", 6: "KW_ERR_INTERNAL"}
 
@@ -316,6 +317,21 @@ def solve(inp: dict, record=("p",), start_index=1, device=-1):
     _check(lib.kw_solve(C.byref(s), C.byref(opt), C.byref(out), C.byref(st)), st)
     del keep
     return to_matlab_layout(bufs, inp)
+
+
+def run_file(input_path, output_path, record=("p",), start_index=1, device=-1, verbose=0):
+    """kw_run_file(): read a k-Wave HDF5 input file, run it, write the output
+    file (what kspaceFirstOrder3DC.m:560-567 does through the binary)."""
+    opt = make_options(record, start_index, device, verbose)
+    st = KwStatus()
+    _check(lib.kw_run_file(os.fsencode(input_path), os.fsencode(output_path), C.byref(opt), C.byref(st)), st)
+
+
+def cli_main(argv):
+    """kw_cli_main(): the command line of the solver binary, in process."""
+    args = [os.fsencode(a) for a in argv]
+    arr = (C.c_char_p * len(args))(*args)
+    return lib.kw_cli_main(len(args), arr)
 
 
 class Session:
