@@ -27,7 +27,7 @@ def test_run_file_3d_matches_solve(tmp_path):
     from kwave import _lib, h5io
 
     record = ("p", "p_max", "p_min", "p_rms", "u", "u_max", "p_final", "u_final", "p_max_all")
-    inp, _, start, meta = case_3d_het(n=(34, 30, 32), nt=50, record=record)
+    inp, _, start, meta = case_3d_het(n=(36, 30, 32), nt=50, record=record)
     fin, fout = tmp_path / "in.h5", tmp_path / "out.h5"
     h5io.write_input_file(fin, inp)
     _lib.run_file(fin, fout, record, start_index=7)
@@ -37,11 +37,11 @@ def test_run_file_3d_matches_solve(tmp_path):
     with h5io.File(fout) as f:
         a = f.attrs("/")
         assert a["file_type"] == "output" and a["major_version"] == "1" and a["minor_version"] == "2"
-        assert int(f.read("/Nx").reshape(-1)[0]) == 34
+        assert int(f.read("/Nx").reshape(-1)[0]) == 36
         assert f.read("/Nx").shape == (1, 1, 1) and f.read("/Nx").dtype == np.uint64
         assert int(f.read("/pml_z_size").reshape(-1)[0]) == int(inp["pml_z_size"])
         assert f.read("/p").shape == (1, 50 - 7 + 1, want["p"].shape[0])
-        assert f.read("/p_final").shape == (32, 30, 34)
+        assert f.read("/p_final").shape == (32, 30, 36)
 
 
 def test_command_line_2d_matches_solve(tmp_path):
