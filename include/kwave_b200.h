@@ -205,6 +205,33 @@ void* kw_session_stream(kw_session* s);
 uint64_t kw_session_launches_per_step(const kw_session* s);
 void kw_session_destroy(kw_session* s);
 
+/*
+ * No counterpart in the reference.
+ *
+ * The k-space staggered gradient of a 2D field, for callers that cannot
+ * allocate device memory: applications that keep all device memory in their
+ * own pool (MATLAB's gpuArray data, a PyTorch caching allocator) or loops
+ * where the device-wide synchronisation a cudaMalloc / cudaFree can cause is
+ * not acceptable.  For f on an nx x ny grid (x fastest) it writes
+ *   gx = real(ifft2(i kx exp(i kx dx/2) kappa fft2(f)))
+ *   gy = real(ifft2(i ky exp(i ky dy/2) kappa fft2(f)))     (d_gy may be NULL)
+ * with kappa = sinc(c_ref |k| dt / 2) -- the gradient kspaceFirstOrder2D.m:920-921
+ * applies to an initial pressure.  d_f, d_gx, d_gy are nx*ny floats of the
+ * current device, owned by the caller.  The call only enqueues work on
+ * `stream` (a cudaStream_t, NULL for the default stream).
+ *
+ * It allocates nothing: its intermediate spectra live in a fixed static
+ * device array sized for edges up to KW_NOALLOC_MAX_EDGE (8 MiB per device);
+ * larger grids are rejected with KW_ERR_INVALID_ARGUMENT.  The first call on
+ * each device does a one-time set-up (looks up that array's address), so
+ * make it before any stream capture.  The array is shared by all calls on a
+ * device: calls that overlap in time on one device race and must be
+ * serialised by the caller.
+ */
+#define KW_NOALLOC_MAX_EDGE 1024
+int kw_kspace_gradient_noalloc(const float* d_f, float* d_gx, float* d_gy, uint64_t nx, uint64_t ny, float dx,
+                               float dy, float c_ref, float dt, void* stream, kw_status* status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,7 +93,7 @@ EXPORTED = [
     "kw_version", "kw_output_sizes_query", "kw_solve", "kw_run_file", "kw_cli_main",
     "kw_session_create", "kw_session_advance", "kw_session_elapsed_ms", "kw_session_sync",
     "kw_session_steps_done", "kw_session_read", "kw_session_stream", "kw_session_launches_per_step",
-    "kw_session_destroy",
+    "kw_session_destroy", "kw_kspace_gradient_noalloc",
 ]
 
 
@@ -122,6 +122,9 @@ def _load():
     lib.kw_session_launches_per_step.argtypes = [C.c_void_p]
     lib.kw_session_launches_per_step.restype = C.c_uint64
     lib.kw_session_destroy.argtypes = [C.c_void_p]
+    lib.kw_kspace_gradient_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                               C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p,
+                                               C.POINTER(KwStatus)]
     return lib
 
 
@@ -387,6 +390,14 @@ class Session:
 
     def __del__(self):
         self.close()
+
+
+def kspace_gradient_noalloc(d_f, d_gx, d_gy, nx, ny, dx, dy, c_ref, dt, stream=None):
+    """kw_kspace_gradient_noalloc(): device pointers (ints) in, nothing
+    allocated; the work is only enqueued on `stream` (a cudaStream_t handle)."""
+    st = KwStatus()
+    _check(lib.kw_kspace_gradient_noalloc(d_f, d_gx, d_gy, int(nx), int(ny), float(dx), float(dy), float(c_ref),
+                                          float(dt), stream, C.byref(st)), st)
 
 
 def version():
