@@ -386,6 +386,48 @@ __device__ __forceinline__ int row_lines(int L) {
 }
 
 // ---------------------------------------------------------------------------
+// L2 prefetch of a row tile's inputs.  Issued when the tile starts, so DRAM
+// streams everything the tile will read while the block is still in its
+// first phase; the later loads then hit L2.  Bulk prefetches need 16-byte
+// aligned addresses and sizes: real fields with nx % 4 == 0 and half-spectrum
+// rows rounded up to an even number of bins (the pitch nxp is a multiple of
+// 32 bins, so the rounded row stays inside it).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+struct TilePrefetch {
+  long long r0;
+  int rows;  // rows of the tile inside [row0, row1)
+  int nx;
+  int nxp;
+  int nxh2;  // half-spectrum bins per row, rounded up to even
+  int slot;  // prefetch slots are dealt to the block's threads round robin
+
+  __device__ TilePrefetch(const Dims& d, long long r, int L)
+      : r0(r), rows((int)min(2LL * L, d.row1 - r)), nx(d.nx), nxp(d.nxp), nxh2((d.nxh + 1) & ~1), slot(0) {}
+  __device__ bool mine() { return (int)threadIdx.x == (slot++ % (int)blockDim.x); }
+  // a real field (x fastest): one contiguous range
+  __device__ void field(const void* f, int elem_bytes = 4) {
+    if (!f || rows <= 0) return;
+    if (mine()) prefetch_l2(static_cast<const char*>(f) + r0 * nx * elem_bytes, (unsigned)rows * nx * elem_bytes);
+  }
+  // a half spectrum: one range per row, padding bins skipped
+  __device__ void spectrum(const float2* S) {
+    if (!S) return;
+    for (int t = 0; t < rows; ++t)
+      if (mine()) prefetch_l2(S + (r0 + t) * nxp, (unsigned)nxh2 * 8u);
+  }
+  __device__ void sensor(const Sensor& s, int fi) {
+    if (s.mode != 1 || fi <= 1) return;
+    field(s.vmax);
+    field(s.vmin);
+    field(s.rms, 8);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // u update: C2R of the gradient, split-PML momentum update, velocity
 // sources, velocity sensors, R2C of the new velocity.  blockIdx.y = axis.
 // ---------------------------------------------------------------------------
@@ -409,6 +451,12 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   const int fi = record_index(a.clk);
   load_c2r<NC>(a.S[ax], B0, lay, d, r0, L, a.kmul[ax]);
   __syncthreads();
+  if constexpr (NC > 0 && NC % 4 == 0) {  // the epilogue's inputs stream in during the FFT
+    TilePrefetch pf(d, r0, L);
+    if (!a.init) pf.field(a.u[ax]);
+    pf.field(a.rinv[ax].p);
+    pf.sensor(a.sens[ax], fi);
+  }
   float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
   float2* W = (G == B0) ? B1 : B0;
   float* u = a.u[ax];
@@ -561,6 +609,19 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, 4) k_x_rho(const __grid_co
     for (int f = 0; f < dim; ++f) {
       load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L);
       __syncthreads();
+      if constexpr (NC % 4 == 0) {  // what the next phase reads streams in during this FFT
+        TilePrefetch pf(d, r0, L);
+        if (f + 1 < dim) {
+          pf.spectrum(a.S[f + 1]);
+        } else {
+          _Pragma("unroll") for (int g = 0; g < dim; ++g) pf.field(a.rho[g]);
+          pf.field(a.rho0.p);
+          pf.field(a.c0sq.p);
+          if (a.nonlinear) pf.field(a.bona.p);
+          if (a.eos == 2) pf.field(a.tau.p);
+          if (a.eos != 1) pf.sensor(a.sens, fi);
+        }
+      }
       tile_fft<NC, true, false>(pool[f], nullptr, tw, plan, L, lay);
     }
     _Pragma("unroll") for (int f = 0; f < dim; ++f) D[f] = pool[f];
@@ -796,6 +857,13 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
   if constexpr (CT) {
     load_c2r<NC>(a.S_b, P1, lay, d, r0, L);
     __syncthreads();
+    if constexpr (NC % 4 == 0) {  // the epilogue's inputs stream in during the FFTs
+      TilePrefetch pf(d, r0, L);
+      pf.field(a.p_loc);
+      pf.field(a.c2tau.p);
+      pf.field(a.c2eta.p);
+      pf.sensor(a.sens, fi);
+    }
 #pragma unroll 1
     for (int f = 0; f < 2; ++f) tile_fft<NC, true, false>(f ? P1 : P0, nullptr, tw, plan, L, lay);
     RA = P0;

@@ -115,12 +115,24 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
   float2* W = inb + 2 * E;                         // product / inverse-transform buffer
   float2* tw = W + E;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + NC);
+  // per-line tables of the transform axis: shifted derivatives (+, -) and k^2
+  float2* dpos = reinterpret_cast<float2*>(bar + 2);
+  float2* dneg = dpos + NC;
+  float* kl2 = reinterpret_cast<float*>(dneg + NC);
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_mbar_init();
   }
-  for (int i = threadIdx.x; i < NC; i += blockDim.x) tw[i] = tw_g[i];
+  const int lax = (a.dim == 3) ? 2 : 1;
+  for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+    tw[i] = tw_g[i];
+    kl2[i] = T.k2[lax][i];
+    if constexpr (CLS == FC_GRAD) {
+      dpos[i] = T.ddk_pos[lax][i];
+      dneg[i] = T.ddk_neg[lax][i];
+    }
+  }
   __syncthreads();
   const int per_in = a.ncx * a.nouter;
   const int ntiles = a.nin * per_in;
@@ -144,7 +156,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
   const ColLayout lay{TL};
   // the line mapping fixes this thread's column (kx) for every pass
   const int l = threadIdx.x % TL, tid = threadIdx.x / TL;
-  const float* kl2 = (a.dim == 3) ? T.k2[2] : T.k2[1];
+  const float cdt2sq = T.cdt2 * T.cdt2;
   int it = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -164,31 +176,32 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
       float e = 0.f;
       if constexpr (CLS == FC_GRAD) {
         if (op.kind != OP_KAPPA) {
-          const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
-          const bool along = (a.dim == 3) ? (op.axis == 2) : (op.axis == 1);
-          if (along)
-            dline = tab;
-          else
+          const bool along = op.axis == lax;
+          if (along) {
+            dline = (op.kind == OP_GRAD_POS) ? dpos : dneg;
+          } else {
+            const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
             dconst = __ldg(tab + (op.axis == 0 ? ix : o));
+          }
         }
       } else if constexpr (CLS == FC_NABLA) {
-        e = (op.kind == OP_NABLA1) ? T.ym2 : T.ym1;
+        e = 0.5f * ((op.kind == OP_NABLA1) ? T.ym2 : T.ym1);  // |k|^y = (|k|^2)^(y/2)
       }
       // W = F * operator (one pass; positions p = tid + k * (TH / TL))
 #pragma unroll 4
       for (int p = tid; p < NC; p += TH / TL) {
-        const float k = sqrtf(kxy2 + __ldg(kl2 + p));
+        const float k2 = kxy2 + kl2[p];
         float m;
         if constexpr (CLS == FC_GRAD) {
-          m = sinc_series(T.cdt2 * k) * T.scale;
+          m = sinc_sq(cdt2sq * k2) * T.scale;
         } else if constexpr (CLS == FC_NABLA) {
-          m = (k == 0.f) ? (e == 0.f ? T.scale : 0.f) : exp2f(e * log2f(k)) * T.scale;
+          m = (k2 == 0.f) ? (e == 0.f ? T.scale : 0.f) : exp2f(e * log2f(k2)) * T.scale;
         } else {
-          m = cos_series(T.cdt2 * k) * T.scale;
+          m = cos_sq(cdt2sq * k2) * T.scale;
         }
         float2 f = F[lay(l, p)];
         f = make_float2(f.x * m, f.y * m);
-        if constexpr (CLS == FC_GRAD) f = c_mul(f, dline ? __ldg(dline + p) : dconst);
+        if constexpr (CLS == FC_GRAD) f = c_mul(f, dline ? dline[p] : dconst);
         W[lay(l, p)] = f;
       }
       __syncthreads();
@@ -280,7 +293,8 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
 
 template <int NC, int CLS>
 static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
-  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t);
+  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 2 * NC * sizeof(float2) +
+                    NC * sizeof(float);
   auto k = k_fused_tma<NC, CLS>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;

@@ -5,42 +5,47 @@
 
 namespace kwb {
 
-// sin(x)/x and cos(x) from their Maclaurin series (Horner form), accurate to
-// FP32 rounding for |x| <= pi; larger arguments use sinf / cosf.
-__device__ __forceinline__ float sinc_series(float x) {
-  const float x2 = x * x;
-  if (x2 > 9.8696044f) return sinf(x) / x;
-  // Horner over sum_{n=0}^{10} (-1)^n x^(2n) / (2n+1)!
-  float s = 1.9572941063391262e-20f;             //  1/21!
-  s = fmaf(s, x2, -8.2206352466243295e-18f);     // -1/19!
-  s = fmaf(s, x2, 2.8114572543455206e-15f);      //  1/17!
-  s = fmaf(s, x2, -7.6471637318198164e-13f);     // -1/15!
-  s = fmaf(s, x2, 1.6059043836821613e-10f);      //  1/13!
-  s = fmaf(s, x2, -2.5052108385441720e-08f);     // -1/11!
-  s = fmaf(s, x2, 2.7557319223985893e-06f);      //  1/9!
-  s = fmaf(s, x2, -1.9841269841269841e-04f);     // -1/7!
-  s = fmaf(s, x2, 8.3333333333333333e-03f);      //  1/5!
-  s = fmaf(s, x2, -1.6666666666666667e-01f);     // -1/3!
-  s = fmaf(s, x2, 1.0f);
+// sin(x)/x and cos(x) from their Maclaurin series (Horner form) as
+// polynomials in u = x^2, so callers holding |k|^2 need no square root.
+// Accurate to FP32 rounding for |x| <= pi; larger arguments use sinf / cosf.
+__device__ __forceinline__ float sinc_sq(float u) {
+  if (u > 9.8696044f) {
+    const float x = sqrtf(u);
+    return sinf(x) / x;
+  }
+  // Horner over sum_{n=0}^{10} (-1)^n u^n / (2n+1)!
+  float s = 1.9572941063391262e-20f;            //  1/21!
+  s = fmaf(s, u, -8.2206352466243295e-18f);     // -1/19!
+  s = fmaf(s, u, 2.8114572543455206e-15f);      //  1/17!
+  s = fmaf(s, u, -7.6471637318198164e-13f);     // -1/15!
+  s = fmaf(s, u, 1.6059043836821613e-10f);      //  1/13!
+  s = fmaf(s, u, -2.5052108385441720e-08f);     // -1/11!
+  s = fmaf(s, u, 2.7557319223985893e-06f);      //  1/9!
+  s = fmaf(s, u, -1.9841269841269841e-04f);     // -1/7!
+  s = fmaf(s, u, 8.3333333333333333e-03f);      //  1/5!
+  s = fmaf(s, u, -1.6666666666666667e-01f);     // -1/3!
+  s = fmaf(s, u, 1.0f);
   return s;
 }
 
-__device__ __forceinline__ float cos_series(float x) {
-  const float x2 = x * x;
-  if (x2 > 9.8696044f) return cosf(x);
-  float s = 4.1103176233121648e-19f;             //  1/20!
-  s = fmaf(s, x2, -1.5619206968586225e-16f);     // -1/18!
-  s = fmaf(s, x2, 4.7794773323873853e-14f);      //  1/16!
-  s = fmaf(s, x2, -1.1470745597729725e-11f);     // -1/14!
-  s = fmaf(s, x2, 2.0876756987868099e-09f);      //  1/12!
-  s = fmaf(s, x2, -2.7557319223985891e-07f);     // -1/10!
-  s = fmaf(s, x2, 2.4801587301587302e-05f);      //  1/8!
-  s = fmaf(s, x2, -1.3888888888888889e-03f);     // -1/6!
-  s = fmaf(s, x2, 4.1666666666666667e-02f);      //  1/4!
-  s = fmaf(s, x2, -0.5f);                        // -1/2!
-  s = fmaf(s, x2, 1.0f);
+__device__ __forceinline__ float cos_sq(float u) {
+  if (u > 9.8696044f) return cosf(sqrtf(u));
+  float s = 4.1103176233121648e-19f;            //  1/20!
+  s = fmaf(s, u, -1.5619206968586225e-16f);     // -1/18!
+  s = fmaf(s, u, 4.7794773323873853e-14f);      //  1/16!
+  s = fmaf(s, u, -1.1470745597729725e-11f);     // -1/14!
+  s = fmaf(s, u, 2.0876756987868099e-09f);      //  1/12!
+  s = fmaf(s, u, -2.7557319223985891e-07f);     // -1/10!
+  s = fmaf(s, u, 2.4801587301587302e-05f);      //  1/8!
+  s = fmaf(s, u, -1.3888888888888889e-03f);     // -1/6!
+  s = fmaf(s, u, 4.1666666666666667e-02f);      //  1/4!
+  s = fmaf(s, u, -0.5f);                        // -1/2!
+  s = fmaf(s, u, 1.0f);
   return s;
 }
+
+__device__ __forceinline__ float sinc_series(float x) { return sinc_sq(x * x); }
+__device__ __forceinline__ float cos_series(float x) { return cos_sq(x * x); }
 
 __device__ __forceinline__ float2 eval_op(const SpecOp& op, const SpecTables& T, int dim, int ix,
                                           int iy, int iz) {
