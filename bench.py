@@ -32,6 +32,10 @@ import time
 
 import numpy as np
 
+# Streams of concurrent simulations (the batched and served samples) need
+# more hardware work queues than the default 8; set before CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "k-wave_b200"))
 sys.path.insert(0, ROOT)
@@ -164,6 +168,95 @@ def cpu_sample(inp, record, steps=3, warmup=2):
     return npts / per, per
 
 
+def batched_sample(n_sims, nt, chunk=25):
+    """Config of many independent 3D linear lossy simulations on uneven
+    2^a 3^b 5^c grids (64..192 per edge): grid-point-steps/s when they advance
+    together (run_batch) and one at a time (the plain drop-in).  Sessions are
+    created before either timed region; each region is bracketed by a device
+    synchronize and timed on the host clock (work on many streams)."""
+    import torch
+
+    from kwave import serving
+    from kwave.simulation import prepare
+    from kwave.workloads import uneven_lossy_3d
+
+    inputs = []
+    for i in range(n_sims):
+        kg, medium, source, sensor = uneven_lossy_3d(i, n_sims=n_sims, nt=nt)
+        inp, record, start, _ = prepare(kg, medium, source, sensor)
+        inputs.append(inp)
+    work = sum(int(i["Nx"]) * int(i["Ny"]) * int(i["Nz"]) * int(i["Nt"]) for i in inputs)
+    res = {}
+    for mode in ("plain", "batched"):
+        sessions = [serving.gpu_session(inp, record) for inp in inputs]
+        for s_ in sessions:
+            s_.sync()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if mode == "plain":
+            for s_, inp in zip(sessions, inputs):
+                s_.advance(int(inp["Nt"]))
+                s_.sync()
+        else:
+            left = [int(i["Nt"]) for i in inputs]
+            while any(left):
+                for k, s_ in enumerate(sessions):
+                    if left[k]:
+                        m = min(chunk, left[k])
+                        s_.advance(m)
+                        left[k] -= m
+            for s_ in sessions:
+                s_.sync()
+        torch.cuda.synchronize()
+        res[mode] = work / (time.perf_counter() - t0)
+        for s_ in sessions:
+            s_.close()
+    return {"workload": f"{n_sims} independent 3D linear lossy sims, edges 64..192 (5-smooth), y 1.1, "
+                        f"200 sensor points, Nt {nt}, FP32", "unit": UNIT,
+            "batched": res["batched"], "plain": res["plain"], "speedup": res["batched"] / res["plain"],
+            "timing": "host clock around a device synchronize; session set-up outside both regions"}
+
+
+def served_sample(n_requests, budget_gb=150.0, chunk=25):
+    """Seeded Poisson stream (20 requests/s) of 2D 256^2..1024^2 and 3D
+    64^3..256^3 solves, half absorbing, Nt 300..1500: time to solution p50 /
+    p99 and aggregate grid-point-steps/s, for the server (admission by
+    device-memory budget, interleaved steps) and for first-come-first-served
+    one-at-a-time solves."""
+    from kwave import serving
+    from kwave.simulation import prepare
+    from kwave.workloads import served_request
+
+    def requests():
+        out = []
+        for i in range(n_requests):
+            arrival, (kg, medium, source, sensor) = served_request(i)
+            inp, record, start, _ = prepare(kg, medium, source, sensor, pml_size=10)
+            out.append(serving.Request(inp=inp, record=tuple(record), arrival=arrival, start_index=start, tag=i))
+        return out
+
+    reqs = requests()
+    srv = serving.Server(budget_bytes=int(budget_gb * 1e9), chunk=chunk)
+    t0 = time.perf_counter()
+    served = srv.serve(reqs)
+    s_served = serving.summary(served, time.perf_counter() - t0)
+    plain_reqs = [serving.Request(inp=r.inp, record=r.record, arrival=r.arrival, start_index=r.start_index, tag=r.tag)
+                  for r in reqs]
+    t0 = time.perf_counter()
+    plain = serving.serve_plain(plain_reqs)
+    s_plain = serving.summary(plain, time.perf_counter() - t0)
+    same = all(np.array_equal(a.result[k], b.result[k]) for a, b in zip(served, plain) for k in a.result)
+    return {"workload": f"{n_requests} requests, Poisson 20/s (seed 5): 2D 256^2..1024^2 / 3D 64^3..256^3, "
+                        "half absorbing (y 1.0-1.8), Nt 300..1500, plane tone-burst source, FP32",
+            "budget_gb": budget_gb, "served": s_served, "plain": s_plain,
+            "p50_speedup": s_plain["p50_s"] / s_served["p50_s"] if s_served["p50_s"] else None,
+            "p99_speedup": s_plain["p99_s"] / s_served["p99_s"] if s_served["p99_s"] else None,
+            "throughput_speedup": (s_served["grid_pt_steps_per_s"] / s_plain["grid_pt_steps_per_s"]
+                                   if s_plain["grid_pt_steps_per_s"] else None),
+            "results_identical": same,
+            "timing": "host clock from the first arrival; latency = finish - arrival"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -212,6 +305,9 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default=None, help="Nx,Ny,Nz for a smaller profiling case (default n^3)")
+    ap.add_argument("--batch-sims", type=int, default=48, help="simulations in the batched sample (0: skip)")
+    ap.add_argument("--batch-nt", type=int, default=100, help="time steps of each batched simulation")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the served sample (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -307,6 +403,11 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                 "sample": f"time steps 3..5 of the same {args.n}^3 run, oracle (numpy/scipy.fft, "
                                           f"all host threads), {per:.2f} s/step"}
+    if rank == 0 and world == 1 and not args.shape:
+        if args.batch_sims > 0:
+            line["batched"] = batched_sample(args.batch_sims, args.batch_nt)
+        if args.serve_requests > 0:
+            line["served"] = served_sample(args.serve_requests)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

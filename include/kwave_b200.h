@@ -197,6 +197,10 @@ int kw_session_elapsed_ms(kw_session* s, float* ms, kw_status* status);
 int kw_session_sync(kw_session* s, kw_status* status);
 /* Steps completed so far. */
 uint64_t kw_session_steps_done(const kw_session* s);
+/* Non-blocking: how many kw_session_advance() calls have steps still
+ * running on the device (0: the session is idle).  What a scheduler that
+ * interleaves many sessions polls instead of blocking in kw_session_sync. */
+int kw_session_query(kw_session* s, uint64_t* in_flight, kw_status* status);
 /* Copy the outputs recorded so far into host buffers. */
 int kw_session_read(kw_session* s, kw_output* out, kw_status* status);
 /* The session's CUDA stream (a cudaStream_t), for event timing by callers. */

@@ -938,6 +938,26 @@ void Session::advance(uint64_t n) {
   last_launches = launches_ - l0;
   last_steps = n;
   ck(cudaEventRecord(ev1, st), "event");
+  cudaEvent_t e = nullptr;
+  if (!spare_ev.empty()) {
+    e = spare_ev.back();
+    spare_ev.pop_back();
+  } else {
+    ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  pending_ev.push_back(e);
+  ck(cudaEventRecord(e, st), "event");
+}
+
+uint64_t Session::in_flight() {
+  while (!pending_ev.empty()) {
+    const cudaError_t q = cudaEventQuery(pending_ev.front());
+    if (q == cudaErrorNotReady) break;
+    ck(q, "cudaEventQuery");
+    spare_ev.push_back(pending_ev.front());
+    pending_ev.pop_front();
+  }
+  return pending_ev.size();
 }
 
 float Session::elapsed_ms() {
@@ -998,6 +1018,8 @@ Session::~Session() {
   if (graph) cudaGraphDestroy(graph);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  for (cudaEvent_t e : pending_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : spare_ev) cudaEventDestroy(e);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -1120,6 +1142,13 @@ int kw_session_sync(kw_session* s, kw_status* status) {
 }
 
 uint64_t kw_session_steps_done(const kw_session* s) { return s ? s->s->t_done : 0; }
+
+int kw_session_query(kw_session* s, uint64_t* in_flight, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s || !in_flight) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL argument");
+    *in_flight = s->s->in_flight();
+  });
+}
 
 int kw_session_read(kw_session* s, kw_output* out, kw_status* status) {
   return guarded(status, [&] {

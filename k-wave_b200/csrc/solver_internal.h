@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <deque>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -35,6 +36,7 @@ class Session {
   void advance(uint64_t n);
   float elapsed_ms();
   void sync();
+  uint64_t in_flight();  // advance() calls whose steps have not finished on the device
   void read(kw_output* out);
   uint64_t last_launches_per_step() const { return last_steps ? last_launches / last_steps : 0; }
   static size_t device_bytes_estimate(const kw_input* in, const kw_options* opt);
@@ -84,6 +86,8 @@ class Session {
   bool p0 = false;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::deque<cudaEvent_t> pending_ev;  // one per advance() still running, oldest first
+  std::vector<cudaEvent_t> spare_ev;
   uint64_t launches_ = 0, last_launches = 0, last_steps = 0;
 
   // operator tables

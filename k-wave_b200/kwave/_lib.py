@@ -93,7 +93,7 @@ EXPORTED = [
     "kw_version", "kw_output_sizes_query", "kw_solve", "kw_run_file", "kw_cli_main",
     "kw_session_create", "kw_session_advance", "kw_session_elapsed_ms", "kw_session_sync",
     "kw_session_steps_done", "kw_session_read", "kw_session_stream", "kw_session_launches_per_step",
-    "kw_session_destroy", "kw_kspace_gradient_noalloc",
+    "kw_session_destroy", "kw_session_query", "kw_kspace_gradient_noalloc",
 ]
 
 
@@ -116,6 +116,7 @@ def _load():
     lib.kw_session_sync.argtypes = [C.c_void_p, C.POINTER(KwStatus)]
     lib.kw_session_steps_done.argtypes = [C.c_void_p]
     lib.kw_session_steps_done.restype = C.c_uint64
+    lib.kw_session_query.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(KwStatus)]
     lib.kw_session_read.argtypes = [C.c_void_p, C.POINTER(KwOutput), C.POINTER(KwStatus)]
     lib.kw_session_stream.argtypes = [C.c_void_p]
     lib.kw_session_stream.restype = C.c_void_p
@@ -368,6 +369,13 @@ class Session:
     @property
     def steps_done(self):
         return int(lib.kw_session_steps_done(self._h))
+
+    def in_flight(self):
+        """How many advance() calls still have steps running on the device."""
+        st = KwStatus()
+        n = C.c_uint64(0)
+        _check(lib.kw_session_query(self._h, C.byref(n), C.byref(st)), st)
+        return int(n.value)
 
     @property
     def stream(self):

@@ -1,0 +1,235 @@
+"""Many independent simulations on one GPU: batched runs and a request server.
+
+The reference runs one simulation per process (``kspaceFirstOrder3DC.m``
+starts the binary once per call), so a GPU holding a small grid sits mostly
+idle.  Here every simulation is a resident session (``kw_session_*``): its
+fields stay in HBM, its time steps are replayed CUDA graphs on its own
+stream, and a host scheduler interleaves the sessions' steps in chunks, so
+kernels of different simulations overlap on the device.  Simulations never
+share device memory, so each result is the same as the same simulation run
+alone.
+
+* :func:`run_batch` advances a fixed set of simulations together;
+* :class:`Server` admits requests as they arrive, while their estimated
+  device memory fits a budget (continuous batching: a request waiting for
+  memory is admitted as soon as a finished one frees enough), and records
+  each request's time to solution.
+
+Both take a ``factory`` that builds a session from a request, so the
+scheduling logic can be exercised without a GPU.
+"""
+from __future__ import annotations
+
+import os
+import time
+from dataclasses import dataclass, field
+
+# More hardware work queues than the default 8, so the streams of many
+# sessions do not serialise behind one another.  Takes effect only if set
+# before the process creates its CUDA context.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+
+def session_bytes(inp, record, sizes):
+    """Device memory a session holds: fields, spectra and medium maps (the
+    library's estimate) plus the recorded outputs."""
+    dim = 2 if int(inp["Nz"]) == 1 else 3
+    ns, nr, ng = int(sizes.num_sensor_points), int(sizes.num_recorded_steps), int(sizes.grid_points)
+    per_series = 4 * ns * nr
+    b = int(sizes.device_bytes)
+    rec = set(record)
+    b += per_series * (("p" in rec) + dim * ("u" in rec) + dim * ("u_non_staggered" in rec))
+    b += 8 * ns * (("p_rms" in rec) + dim * ("u_rms" in rec)) + 4 * ns * 4
+    b += 4 * ng * sum(k in rec for k in ("p_max_all", "p_min_all", "p_final"))
+    b += 4 * ng * dim * sum(k in rec for k in ("u_max_all", "u_min_all", "u_final"))
+    return b
+
+
+def gpu_session(inp, record, start_index=1, device=-1):
+    from ._lib import Session
+
+    return Session(inp, record, start_index, device)
+
+
+@dataclass
+class Request:
+    """One simulation request: the input datasets, what to record, and when
+    it arrives (seconds after the server starts)."""
+    inp: dict
+    record: tuple = ("p",)
+    arrival: float = 0.0
+    start_index: int = 1
+    tag: object = None
+    # filled in by the server
+    admitted: float = None
+    finished: float = None
+    result: dict = None
+    error: str = None
+    nbytes: int = 0
+
+    @property
+    def latency(self):
+        return None if self.finished is None else self.finished - self.arrival
+
+    @property
+    def grid_point_steps(self):
+        return int(self.inp["Nx"]) * int(self.inp["Ny"]) * int(self.inp["Nz"]) * int(self.inp["Nt"])
+
+
+def run_batch(inputs, record=("p",), chunk=25, factory=gpu_session, sync=True):
+    """Advance every simulation in `inputs` to its last step, interleaving
+    them in chunks of `chunk` steps, and return their outputs in order.
+
+    Work is only enqueued here (each session's steps go to its own stream),
+    so the device runs the simulations concurrently."""
+    sessions = [factory(inp, record) for inp in inputs]
+    try:
+        left = [int(inp["Nt"]) for inp in inputs]
+        while any(left):
+            for i, s in enumerate(sessions):
+                if left[i]:
+                    n = min(chunk, left[i])
+                    s.advance(n)
+                    left[i] -= n
+        return [s.read() for s in sessions] if sync else sessions
+    finally:
+        if sync:
+            for s in sessions:
+                s.close()
+
+
+def run_plain(inputs, record=("p",), factory=gpu_session):
+    """The one-simulation-at-a-time drop-in: each simulation runs to its end
+    before the next starts."""
+    out = []
+    for inp in inputs:
+        s = factory(inp, record)
+        try:
+            s.advance(int(inp["Nt"]))
+            out.append(s.read())
+        finally:
+            s.close()
+    return out
+
+
+def library_sizer(r):
+    """Device bytes of a request, from the library's output-size query."""
+    from ._lib import make_input, make_options, output_sizes
+
+    s, keep = make_input(r.inp)
+    return session_bytes(r.inp, r.record, output_sizes(s, make_options(r.record, r.start_index)))
+
+
+@dataclass
+class Server:
+    """Admits requests by device-memory budget and interleaves their steps.
+
+    `budget_bytes` bounds the summed estimate of admitted sessions;
+    `chunk` is the number of steps queued per session per call; a session
+    gets its next chunk while fewer than `max_queued` of its chunks are
+    still running, so its stream never runs dry while the host is busy
+    elsewhere.  `clock` / `sleep` are the time source (replaceable by a
+    simulated clock in tests)."""
+    budget_bytes: int = 150 * 10**9
+    chunk: int = 25
+    max_queued: int = 2
+    factory: object = gpu_session
+    sizer: object = library_sizer
+    clock: object = time.perf_counter
+    sleep: object = time.sleep
+    idle_sleep_s: float = 2e-4
+    log: list = field(default_factory=list)
+
+    def serve(self, requests):
+        """Run `requests` to completion in arrival order; returns them with
+        admitted / finished times (seconds after start) and results."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        for r in pending:
+            r.nbytes = int(self.sizer(r))
+            if r.nbytes > self.budget_bytes:
+                r.error = f"needs {r.nbytes} B of device memory, more than the {self.budget_bytes} B budget"
+        queue = [r for r in pending if r.error is None]
+        active = []  # [request, session, steps queued]
+        used = 0
+        t0 = self.clock()
+        now = lambda: self.clock() - t0
+        while queue or active:
+            progressed = False
+            # admission: arrived requests, first come first served, while they fit
+            while queue and queue[0].arrival <= now() and used + queue[0].nbytes <= self.budget_bytes:
+                r = queue.pop(0)
+                try:
+                    sess = self.factory(r.inp, r.record, r.start_index)
+                except Exception as e:  # noqa: BLE001 - reported per request
+                    r.error = str(e)
+                    continue
+                r.admitted = now()
+                used += r.nbytes
+                active.append([r, sess, 0])
+                self.log.append(("admit", r.tag, r.admitted, used))
+                progressed = True
+            # interleave: top up each session's stream with its next chunk,
+            # collect the sessions whose last step has finished
+            for a in list(active):
+                r, sess, queued = a
+                nt = int(r.inp["Nt"])
+                if queued < nt:
+                    if sess.in_flight() < self.max_queued:
+                        n = min(self.chunk, nt - queued)
+                        sess.advance(n)
+                        a[2] = queued + n
+                        self.log.append(("advance", r.tag, now(), n))
+                        progressed = True
+                elif sess.in_flight() == 0:
+                    try:
+                        r.result = sess.read()
+                    except Exception as e:  # noqa: BLE001
+                        r.error = str(e)
+                    finally:
+                        sess.close()
+                    r.finished = now()
+                    used -= r.nbytes
+                    active.remove(a)
+                    self.log.append(("finish", r.tag, r.finished, used))
+                    progressed = True
+            if not progressed:
+                self.sleep(self.idle_sleep_s)
+        return pending
+
+
+def serve_plain(requests, factory=gpu_session, clock=time.perf_counter, sleep=time.sleep):
+    """First come, first served, one simulation at a time (the plain drop-in
+    behind a queue): the baseline for the server's latencies."""
+    pending = sorted(requests, key=lambda r: r.arrival)
+    t0 = clock()
+    for r in pending:
+        while clock() - t0 < r.arrival:
+            sleep(min(1e-3, r.arrival - (clock() - t0)))
+        r.admitted = clock() - t0
+        sess = factory(r.inp, r.record, r.start_index)
+        try:
+            sess.advance(int(r.inp["Nt"]))
+            r.result = sess.read()
+        finally:
+            sess.close()
+        r.finished = clock() - t0
+    return pending
+
+
+def percentile(values, q):
+    v = sorted(values)
+    if not v:
+        return None
+    k = (len(v) - 1) * q / 100.0
+    lo, hi = int(k), min(int(k) + 1, len(v) - 1)
+    return v[lo] + (v[hi] - v[lo]) * (k - lo)
+
+
+def summary(requests, elapsed_s=None):
+    done = [r for r in requests if r.finished is not None and r.error is None]
+    lat = [r.latency for r in done]
+    span = elapsed_s if elapsed_s is not None else (max(r.finished for r in done) if done else 0.0)
+    gps = sum(r.grid_point_steps for r in done)
+    return {"requests": len(requests), "completed": len(done), "failed": sum(r.error is not None for r in requests),
+            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "mean_s": sum(lat) / len(lat) if lat else None,
+            "makespan_s": span, "grid_pt_steps_per_s": gps / span if span else None}

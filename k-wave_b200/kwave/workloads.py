@@ -101,3 +101,63 @@ def uneven_lossy_3d(index, n_sims=48, nt=500, dx=1e-4, n_sensors=200, seed=4):
     mask[r2.choice(mask.size, n_sensors, replace=False)] = 1
     sensor = {"mask": mask.reshape(shape, order="F"), "record": ["p"]}
     return kgrid, medium, {"p0": p0}, sensor
+
+
+def five_smooth(lo, hi):
+    """Integers in [lo, hi] with no prime factor above 5 (FFT-friendly edges)."""
+    out = []
+    for n in range(lo, hi + 1):
+        m = n
+        for p in (2, 3, 5):
+            while m % p == 0:
+                m //= p
+        if m == 1:
+            out.append(n)
+    return tuple(out)
+
+
+EDGES_2D = five_smooth(256, 1024)
+EDGES_3D = five_smooth(64, 256)
+
+
+def served_request(index, seed=5, rate=20.0, dx=1e-4, pml=10, n_sensors=64):
+    """The `index`-th request of a seeded Poisson stream (mean `rate` per
+    second): arrival time plus (kgrid, medium, source, sensor).  Half are 2D
+    (edges 256..1024), half 3D (edges 64..256), all 2^a 3^b 5^c; half
+    lossless, half power-law absorbing with y in U[1.0, 1.8] (y = 1 exactly
+    is excluded, as the reference rejects it); smoothed random media; a
+    plane pressure source driven by a tone burst; Nt in U[300, 1500]."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=index + 1)
+    arrival = float(np.cumsum(gaps)[index])
+    r = np.random.default_rng(seed * 100003 + index)
+    three_d = bool(r.integers(0, 2))
+    edges = EDGES_3D if three_d else EDGES_2D
+    n = int(r.choice(edges))
+    dim = 3 if three_d else 2
+    shape = (n,) * dim
+    absorbing = bool(r.integers(0, 2))
+    alpha_power = float(r.uniform(1.0, 1.8))
+    if abs(alpha_power - 1.0) < 1e-3:
+        alpha_power = 1.001
+    nt = int(r.integers(300, 1501))
+    zc = smoothed_noise(shape, seed * 100003 + index + 1)
+    zr = smoothed_noise(shape, seed * 100003 + index + 2)
+    c = 1500.0 + 40.0 * zc
+    rho = 1000.0 + 30.0 * zr
+    kgrid = KWaveGrid(shape, (dx,) * dim)
+    dt = 0.3 * dx / c.max()
+    kgrid.set_time(nt, dt)
+    medium = {"sound_speed": c, "density": rho}
+    if absorbing:
+        medium.update(alpha_coeff=0.75, alpha_power=alpha_power)
+    mask = np.zeros(shape)
+    if three_d:
+        mask[pml + 1, pml:n - pml, pml:n - pml] = 1
+    else:
+        mask[pml + 1, pml:n - pml] = 1
+    source = {"p_mask": mask, "p": 1e5 * tone_burst(1.0 / dt, 1e6, 3), "p_mode": "additive"}
+    smask = np.zeros(int(np.prod(shape)))
+    smask[r.choice(smask.size, n_sensors, replace=False)] = 1
+    sensor = {"mask": smask.reshape(shape, order="F"), "record": ["p"]}
+    return arrival, (kgrid, medium, source, sensor)

@@ -1,0 +1,150 @@
+"""The batch runner and request server's scheduling, without a GPU: fake
+sessions whose chunks take simulated time on a simulated clock."""
+import numpy as np
+import pytest
+
+from kwave import serving
+
+
+class Clock:
+    def __init__(self):
+        self.t = 0.0
+
+    def now(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += dt
+
+
+class FakeSession:
+    """Each chunk of n steps occupies the session's stream for n * cost
+    simulated seconds; sessions run side by side."""
+
+    def __init__(self, clock, inp, record, start_index=1, cost=1e-3, trace=None):
+        self.clock, self.inp, self.cost = clock, inp, cost
+        self.ends = []
+        self.steps = 0
+        self.closed = False
+        self.trace = trace if trace is not None else []
+
+    def advance(self, n):
+        start = max([self.clock.now()] + self.ends[-1:])
+        self.ends.append(start + n * self.cost)
+        self.steps += n
+        self.trace.append((self.inp["tag"], n))
+
+    def in_flight(self):
+        return sum(e > self.clock.now() for e in self.ends)
+
+    def read(self):
+        assert self.steps == self.inp["Nt"] and self.in_flight() == 0
+        return {"p": np.full(3, float(self.inp["tag"]))}
+
+    def close(self):
+        self.closed = True
+
+
+def _req(tag, nt=100, arrival=0.0, nbytes=1):
+    return serving.Request(inp={"Nx": 4, "Ny": 4, "Nz": 1, "Nt": nt, "tag": tag, "bytes": nbytes}, arrival=arrival,
+                           tag=tag)
+
+
+def _server(clock, budget, trace=None, chunk=10):
+    made = []
+
+    def factory(inp, record, start_index=1):
+        s = FakeSession(clock, inp, record, start_index, trace=trace)
+        made.append(s)
+        return s
+
+    srv = serving.Server(budget_bytes=budget, chunk=chunk, factory=factory, sizer=lambda r: r.inp["bytes"],
+                         clock=clock.now, sleep=clock.sleep, idle_sleep_s=1e-4)
+    return srv, made
+
+
+def test_budget_bounds_the_admitted_sessions_and_order_is_fifo():
+    clock = Clock()
+    srv, made = _server(clock, budget=2)
+    reqs = [_req(i) for i in range(5)]
+    out = srv.serve(reqs)
+    assert all(r.error is None and r.result is not None for r in out)
+    assert all(int(r.result["p"][0]) == r.tag for r in out)
+    assert all(s.closed for s in made)
+    admits = [e for e in srv.log if e[0] == "admit"]
+    assert [e[1] for e in admits] == [0, 1, 2, 3, 4]
+    assert max(e[3] for e in admits) <= 2
+    # with room for two, the third waits for the first to finish
+    fin = {e[1]: e[2] for e in srv.log if e[0] == "finish"}
+    assert dict((e[1], e[2]) for e in admits)[2] >= min(fin[0], fin[1])
+
+
+def test_oversized_request_is_rejected_and_the_rest_complete():
+    clock = Clock()
+    srv, _ = _server(clock, budget=3)
+    reqs = [_req(0), _req(1, nbytes=4), _req(2)]
+    out = srv.serve(reqs)
+    assert out[1].error and "budget" in out[1].error and out[1].result is None
+    assert out[0].result is not None and out[2].result is not None
+
+
+def test_steps_of_active_sessions_interleave():
+    clock = Clock()
+    trace = []
+    srv, _ = _server(clock, budget=10, trace=trace)
+    srv.serve([_req(0, nt=100), _req(1, nt=100)])
+    first = [t for t, _ in trace[:6]]
+    assert set(first) == {0, 1}  # both progress before either finishes
+    # a session never has more than max_queued chunks running
+    assert sum(n for t, n in trace if t == 0) == 100
+
+
+def test_late_request_is_admitted_while_a_long_one_runs():
+    clock = Clock()
+    srv, _ = _server(clock, budget=10)
+    reqs = [_req(0, nt=2000), _req(1, nt=50, arrival=0.05)]
+    out = srv.serve(reqs)
+    long, short = out
+    assert short.admitted >= 0.05 and short.admitted < long.finished
+    assert short.finished < long.finished
+    assert short.latency < 0.5 * long.latency
+
+
+def test_admission_waits_for_arrival_times():
+    clock = Clock()
+    srv, _ = _server(clock, budget=10)
+    reqs = [_req(i, nt=10, arrival=0.1 * i) for i in range(4)]
+    out = srv.serve(reqs)
+    for r in out:
+        assert r.admitted >= r.arrival - 1e-12
+        assert r.finished > r.admitted
+
+
+def test_batch_and_plain_return_outputs_in_order():
+    clock = Clock()
+    mk = lambda inp, record, start_index=1: FakeSession(clock, inp, record, cost=0.0)
+    inputs = [{"Nx": 4, "Ny": 4, "Nz": 1, "Nt": nt, "tag": i} for i, nt in enumerate((30, 7, 55))]
+    a = serving.run_batch(inputs, ("p",), chunk=10, factory=mk)
+    b = serving.run_plain(inputs, ("p",), factory=mk)
+    assert [int(x["p"][0]) for x in a] == [0, 1, 2] == [int(x["p"][0]) for x in b]
+
+
+def test_summary_percentiles():
+    reqs = [_req(i) for i in range(5)]
+    for i, r in enumerate(reqs):
+        r.finished = 1.0 + i
+    s = serving.summary(reqs)
+    assert s["completed"] == 5 and s["p50_s"] == pytest.approx(3.0) and s["p99_s"] == pytest.approx(4.96)
+    assert serving.percentile([], 50) is None
+
+
+def test_session_bytes_counts_recorded_outputs():
+    class Sz:
+        num_sensor_points, num_recorded_steps, grid_points, device_bytes = 10, 100, 1000, 5000
+
+    inp = {"Nz": 1}
+    base = serving.session_bytes(inp, ("p_max",), Sz)
+    assert serving.session_bytes(inp, ("p",), Sz) - serving.session_bytes(inp, (), Sz) == 4 * 10 * 100
+    assert serving.session_bytes(inp, ("u",), Sz) - serving.session_bytes(inp, (), Sz) == 2 * 4 * 10 * 100
+    assert serving.session_bytes(inp, ("p_final",), Sz) - serving.session_bytes(inp, (), Sz) == 4 * 1000
+    assert base >= 5000
