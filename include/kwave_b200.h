@@ -201,6 +201,14 @@ uint64_t kw_session_steps_done(const kw_session* s);
  * running on the device (0: the session is idle).  What a scheduler that
  * interleaves many sessions polls instead of blocking in kw_session_sync. */
 int kw_session_query(kw_session* s, uint64_t* in_flight, kw_status* status);
+/* CUDA stream priorities of the current device: `least` is the default and
+ * lowest, `greatest` (numerically smaller) the highest. */
+int kw_stream_priority_range(int* least, int* greatest);
+/* Run the session's work at a CUDA stream priority (clamped to the device's
+ * range).  Waits for the session's queued work first.  A scheduler gives the
+ * shortest jobs the highest priority: their kernels go first and longer
+ * jobs' kernels fill the SMs they leave idle. */
+int kw_session_set_priority(kw_session* s, int priority, kw_status* status);
 /* Copy the outputs recorded so far into host buffers. */
 int kw_session_read(kw_session* s, kw_output* out, kw_status* status);
 /* The session's CUDA stream (a cudaStream_t), for event timing by callers. */

@@ -51,11 +51,41 @@ def _run(cmd):
     return r
 
 
-def build(force: bool = False, jobs: int = 4, verbose: bool = False) -> str:
+def ct_sizes():
+    """Transform lengths listed in csrc/ct_sizes.h."""
+    import re
+
+    with open(os.path.join(CSRC, "ct_sizes.h")) as f:
+        return [int(v) for v in re.findall(r"X\((\d+)\)", f.read())]
+
+
+def _ct_sources():
+    """One generated translation unit per compile-time length: an explicit
+    instantiation of CtKernels<N> (kernels_impl.cuh)."""
+    d = os.path.join(BUILD, "ct")
+    os.makedirs(d, exist_ok=True)
+    out = []
+    for n in ct_sizes():
+        path = os.path.join(d, f"kernels_ct_{n}.cu")
+        text = f'#include "kernels_impl.cuh"\nnamespace kwb {{\ntemplate struct CtKernels<{n}>;\n}}\n'
+        if not os.path.exists(path) or open(path).read() != text:
+            with open(path, "w") as f:
+                f.write(text)
+        out.append(path)
+    return out
+
+
+def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    jobs = jobs or os.cpu_count() or 4
     hdrs = _headers()
     jobs_list = []
     objs = []
+    for s in _ct_sources():
+        o = s[:-3] + ".o"
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            jobs_list.append([NVCC] + ARCH + CU_FLAGS + ["-c", s, "-o", o])
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
@@ -84,6 +114,6 @@ def build(force: bool = False, jobs: int = 4, verbose: bool = False) -> str:
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
-    ap.add_argument("--jobs", type=int, default=4)
+    ap.add_argument("--jobs", type=int, default=0, help="parallel compiles (0: one per CPU)")
     a = ap.parse_args()
     print(build(force=a.force, jobs=a.jobs, verbose=True))

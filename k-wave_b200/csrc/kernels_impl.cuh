@@ -1,0 +1,1144 @@
+// Solver kernels: per-axis FFT passes fused with the k-space operators and
+// the split-field PML / conservation updates of k-Wave's fluid time loop
+// (k-Wave/kspaceFirstOrder3D.m:767-1206, kspaceFirstOrder2D.m:710-1042).
+//
+// One time step is a pipeline of three spectral operations, each a forward
+// transform, a k-space multiply and inverse transform(s):
+//   grad p   -> u update          (kspaceFirstOrder3D.m:790-801)
+//   div u    -> rho update, EOS   (:905-925, :963-1017)
+//   absorption (power-law EOS)    (:970-977)
+// The x axis is always the first forward / last inverse transform and is
+// done by the row kernels (k_x_*), which fuse C2R -> elementwise physics ->
+// R2C so each field row is read and written once.  The y axis (3D) is a
+// column pass (k_col_fft) and the last axis (z in 3D, y in 2D) is done by
+// k_fused_last: forward, operator multiply, inverse, in one kernel.
+//
+// Every FFT-carrying kernel is a template on NC, the length of the axis it
+// transforms: NC > 0 selects the compile-time engine (fft_ct.cuh: in-place
+// register-staged stages, one shared-memory buffer per field, index math
+// folded to constants); NC == 0 is the runtime-plan engine for any other
+// 2^a 3^b 5^c length.
+#pragma once
+#include "fft_ct.cuh"
+#include "kernels.cuh"
+#include "spec_ops.cuh"
+
+namespace kwb {
+
+// Lines per block / threads per block of a kernel instantiation.
+template <int NC>
+struct Tile {
+  static constexpr int LINES = ct_lines_of(NC);
+  static constexpr int THREADS = NC > 0 ? ct_threads_of(NC) : kThreads;
+};
+// Row (x) tiles use half as many lines: smaller blocks, more of them per SM,
+// so their load / transform / store phases overlap.
+template <int NC>
+struct RTile {
+  static constexpr int LINES = NC > 0 ? (ct_lines_of(NC) / 2 > 0 ? ct_lines_of(NC) / 2 : 1) : 0;
+  static constexpr int THREADS = NC > 0 ? (NC / ct_rmax(NC)) * LINES : kThreads;
+  // blocks per SM the register budget is sized for (about 512 threads)
+  static constexpr int MIN_BLOCKS = THREADS <= 128 ? 4 : (THREADS <= 256 ? 2 : 1);
+};
+
+// Transform the lines of a tile.  Compile-time lengths run in place in `a`;
+// the runtime engine ping-pongs with `b`.  Returns the result buffer.
+template <int NC, bool INV, bool COL, class L>
+__device__ __forceinline__ float2* tile_fft(float2* a, float2* b, const float2* __restrict__ tw,
+                                            const FFTPlan& plan, int nlines, L lay) {
+  if constexpr (NC > 0) {
+    ct_fft<NC, INV, COL, Tile<NC>::LINES>(a, tw, lay);
+    return a;
+  } else {
+    return fft_lines<INV, COL>(a, b, tw, plan, nlines, lay);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// column passes
+// ---------------------------------------------------------------------------
+template <int NC, bool INV>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_col_fft(ColArgs a, const __grid_constant__ FFTPlan plan,
+                                                               const float2* __restrict__ tw_g) {
+  extern __shared__ float2 sm[];
+  constexpr bool CT = NC > 0;
+  const int n = CT ? NC : plan.n;
+  const int tl = CT ? Tile<NC>::LINES : a.tl;
+  float2* tw = sm;
+  float2* b0 = sm + n;
+  float2* b1 = CT ? nullptr : b0 + tl * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
+  float2* g = a.buf[blockIdx.z] + (long long)(a.outer0 + blockIdx.y) * a.ostride;
+  const int c0 = blockIdx.x * tl;
+  const int total = tl * n;
+#pragma unroll 4
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int l = i % tl, p = i / tl, c = c0 + l;
+    b0[i] = (c < a.ncols) ? g[p * a.lstride + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* r = tile_fft<NC, INV, true>(b0, b1, tw, plan, tl, ColLayout{tl});
+#pragma unroll 4
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int l = i % tl, p = i / tl, c = c0 + l;
+    if (c < a.ncols) g[p * a.lstride + c] = r[i];
+  }
+}
+
+// Last axis: forward transform, multiply by `fanout` operators, inverse
+// transform each product.
+template <int NC>
+__global__ void __launch_bounds__(Tile<NC>::THREADS) k_fused_last(const __grid_constant__ FusedArgs a,
+                                                                  const __grid_constant__ FFTPlan plan,
+                                                                  const float2* __restrict__ tw_g,
+                                                                  const __grid_constant__ SpecTables T, int dim) {
+  extern __shared__ float2 sm[];
+  constexpr bool CT = NC > 0;
+  const int n = CT ? NC : plan.n;
+  const int tl = CT ? Tile<NC>::LINES : a.tl;
+  float2* tw = sm;
+  float2* A = sm + n;
+  float2* B = A + tl * n;
+  float2* C = CT ? nullptr : B + tl * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_g[i];
+  const int g = blockIdx.z;
+  const int outer = blockIdx.y;
+  const long long off = (long long)outer * a.ostride;
+  const float2* src = a.in[g] + off;
+  const int c0 = blockIdx.x * tl;
+  const int total = tl * n;
+#pragma unroll 4
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int l = i % tl, p = i / tl, c = c0 + l;
+    A[i] = (c < a.ncols) ? src[p * a.lstride + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const ColLayout lay{tl};
+  float2* F = tile_fft<NC, false, true>(A, B, tw, plan, tl, lay);
+  float2* W1 = (F == A) ? B : A;
+  float2* W2 = C;
+  for (int o = 0; o < a.fanout; ++o) {
+    const SpecOp op = a.op[g * a.fanout + o];
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int l = i % tl, p = i / tl;
+      int c = c0 + l;
+      if (c >= a.ncols) c = 0;
+      const int iy = (dim == 3) ? outer : p;
+      const int iz = (dim == 3) ? p : 0;
+      W1[i] = c_mul(F[i], eval_op(op, T, dim, c, iy, iz));
+    }
+    __syncthreads();
+    float2* R = tile_fft<NC, true, true>(W1, W2, tw, plan, tl, lay);
+    float2* dst = a.out[g * a.fanout + o] + off;
+    float2* dst2 = a.dual_out[g * a.fanout + o];
+    const float2 dsc = dst2 ? __ldg(a.dual_tab[g * a.fanout + o] + outer) : make_float2(0.f, 0.f);
+    if (dst2) dst2 += off;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int l = i % tl, p = i / tl, c = c0 + l;
+      if (c < a.ncols) {
+        dst[p * a.lstride + c] = R[i];
+        if (dst2) dst2[p * a.lstride + c] = c_mul(R[i], dsc);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// row (x axis) helpers.  A row tile holds 2L consecutive rows packed two per
+// complex line (row 2l in the real part, row 2l+1 in the imaginary part).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float get_comp(const float2* b, RowLayout lay, int q, int x) {
+  const float2& v = b[lay(q >> 1, x)];
+  return (q & 1) ? v.y : v.x;
+}
+__device__ __forceinline__ void set_comp(float2* b, RowLayout lay, int q, int x, float v) {
+  float* f = reinterpret_cast<float*>(b + lay(q >> 1, x));
+  f[q & 1] = v;
+}
+
+// Build the full complex spectrum of each packed line from two half spectra
+// (C2R).  The imaginary parts of the k = 0 and Nyquist bins are dropped,
+// which is the Hermitian projection that real(ifftn(.)) performs.
+template <int NC>
+__device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* buf, RowLayout lay, const Dims& d,
+                                         long long r0, int L, const float2* __restrict__ kmul = nullptr) {
+  if constexpr (NC > 0 && NC % 4 == 0) {
+    // paired 16-byte loads; each loaded bin k also fills its mirror n - k
+    constexpr int n = NC, np = NC / 4 + 1;  // bin pairs (k, k+1), k even, k <= n/2
+    const int total = L * np;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int l = i / np, k = 2 * (i - l * np);
+      const long long ra = r0 + 2 * l, rb = ra + 1;
+      float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
+      if (ra < d.row1) A = *reinterpret_cast<const float4*>(S + ra * d.nxp + k);
+      if (rb < d.row1) B = *reinterpret_cast<const float4*>(S + rb * d.nxp + k);
+      if (kmul) {
+        const float2 m0 = __ldg(kmul + k), m1 = __ldg(kmul + min(k + 1, n / 2));
+        float2 t = c_mul(make_float2(A.x, A.y), m0), u = c_mul(make_float2(A.z, A.w), m1);
+        A = make_float4(t.x, t.y, u.x, u.y);
+        t = c_mul(make_float2(B.x, B.y), m0);
+        u = c_mul(make_float2(B.z, B.w), m1);
+        B = make_float4(t.x, t.y, u.x, u.y);
+      }
+      if (k == 0) {
+        A.y = 0.f;
+        B.y = 0.f;
+      }
+      if (2 * k == n) {
+        A.y = 0.f;
+        B.y = 0.f;
+      }
+      buf[lay(l, k)] = make_float2(A.x - B.y, A.y + B.x);
+      if (k > 0 && 2 * k < n) buf[lay(l, n - k)] = make_float2(A.x + B.y, B.x - A.y);
+      if (2 * (k + 1) < n) {
+        buf[lay(l, k + 1)] = make_float2(A.z - B.w, A.w + B.z);
+        buf[lay(l, n - k - 1)] = make_float2(A.z + B.w, B.z - A.w);
+      }
+    }
+    return;
+  }
+  const int n = NC > 0 ? NC : d.nx;
+  const int total = L * n;
+#pragma unroll 4
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int l = i / n, k = i - l * n;
+    const long long ra = r0 + 2 * l, rb = ra + 1;
+    const int kk = (2 * k <= n) ? k : n - k;
+    float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+    if (ra < d.row1) A = S[ra * d.nxp + kk];
+    if (rb < d.row1) B = S[rb * d.nxp + kk];
+    if (kmul) {
+      const float2 m = __ldg(kmul + kk);
+      A = c_mul(A, m);
+      B = c_mul(B, m);
+    }
+    if (2 * k > n) {
+      A.y = -A.y;
+      B.y = -B.y;
+    } else if (k == 0 || 2 * k == n) {
+      A.y = 0.f;
+      B.y = 0.f;
+    }
+    buf[lay(l, k)] = make_float2(A.x - B.y, A.y + B.x);
+  }
+}
+
+// Split each packed line's spectrum Z = FFT(a + i b) into the half spectra
+// of a and b (R2C) and store them.
+template <int NC>
+__device__ __forceinline__ void store_r2c(const float2* buf, float2* __restrict__ S, RowLayout lay, const Dims& d,
+                                          long long r0, int L) {
+  if constexpr (NC > 0 && NC % 4 == 0) {
+    constexpr int n = NC, nh = NC / 2 + 1, np = NC / 4 + 1;
+    const int total = L * np;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int l = i / np, k = 2 * (i - l * np);
+      const long long ra = r0 + 2 * l, rb = ra + 1;
+      const float2 z0 = buf[lay(l, k)], m0 = buf[lay(l, k == 0 ? 0 : n - k)];
+      const float2 z1 = buf[lay(l, k + 1)], m1 = buf[lay(l, n - k - 1)];
+      const float4 A = make_float4(0.5f * (z0.x + m0.x), 0.5f * (z0.y - m0.y), 0.5f * (z1.x + m1.x),
+                                   0.5f * (z1.y - m1.y));
+      const float4 B = make_float4(0.5f * (z0.y + m0.y), -0.5f * (z0.x - m0.x), 0.5f * (z1.y + m1.y),
+                                   -0.5f * (z1.x - m1.x));
+      if (k + 1 < nh) {
+        if (ra < d.row1) *reinterpret_cast<float4*>(S + ra * d.nxp + k) = A;
+        if (rb < d.row1) *reinterpret_cast<float4*>(S + rb * d.nxp + k) = B;
+      } else {
+        if (ra < d.row1) S[ra * d.nxp + k] = make_float2(A.x, A.y);
+        if (rb < d.row1) S[rb * d.nxp + k] = make_float2(B.x, B.y);
+      }
+    }
+    return;
+  }
+  const int n = NC > 0 ? NC : d.nx;
+  const int nh = n / 2 + 1;
+  const int total = L * nh;
+#pragma unroll 4
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int l = i / nh, k = i - l * nh;
+    const long long ra = r0 + 2 * l, rb = ra + 1;
+    const float2 zk = buf[lay(l, k)];
+    const float2 zn = buf[lay(l, k == 0 ? 0 : n - k)];
+    const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+    const float2 B = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+    if (ra < d.row1) S[ra * d.nxp + k] = A;
+    if (rb < d.row1) S[rb * d.nxp + k] = B;
+  }
+}
+
+__device__ __forceinline__ int lower_bound_i(const int* a, int n, long long v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((long long)__ldg(a + mid) < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Range [lo, hi) of sorted indices that fall inside the tile's rows.
+__device__ __forceinline__ void tile_range(const int* idx, int n, long long a, long long b, int* sh) {
+  if (threadIdx.x == 0) {
+    sh[0] = lower_bound_i(idx, n, a);
+    sh[1] = lower_bound_i(idx, n, b);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void sensor_put(const Sensor& s, int fi, long long slot, float v) {
+  if (s.raw) s.raw[(long long)(fi - 1) * s.ns + slot] = v;
+  if (s.vmax) s.vmax[slot] = (fi == 1) ? v : fmaxf(s.vmax[slot], v);
+  if (s.vmin) s.vmin[slot] = (fi == 1) ? v : fminf(s.vmin[slot], v);
+  if (s.rms) {
+    // compensated (Kahan) running sum of squares
+    float2 acc = (fi == 1) ? make_float2(0.f, 0.f) : s.rms[slot];
+    const float y = v * v - acc.y;
+    const float t = acc.x + y;
+    acc.y = (t - acc.x) - y;
+    acc.x = t;
+    s.rms[slot] = acc;
+  }
+}
+
+__device__ __forceinline__ void sensor_all(const Sensor& s, int fi, long long gi, float v) {
+  if (s.max_all) s.max_all[gi] = (fi == 1) ? v : fmaxf(s.max_all[gi], v);
+  if (s.min_all) s.min_all[gi] = (fi == 1) ? v : fminf(s.min_all[gi], v);
+}
+
+__device__ __forceinline__ int record_index(const Clock& c) {
+  const int t = *c.t;
+  return (t >= c.start) ? (t - c.start + 1) : 0;
+}
+
+// Dense sensors for one grid point (mode 1) and full-grid reductions.
+__device__ __forceinline__ void sensor_dense(const Sensor& s, int fi, long long gi, float v) {
+  if (fi <= 0) return;
+  if (s.mode == 1) sensor_put(s, fi, gi, v);
+  sensor_all(s, fi, gi, v);
+}
+
+// ----- 4-wide (16-byte) variants for the compile-time path -----
+__device__ __forceinline__ float4 ld4(const float* p, long long i) { return *reinterpret_cast<const float4*>(p + i); }
+__device__ __forceinline__ void st4(float* p, long long i, float4 v) { *reinterpret_cast<float4*>(p + i) = v; }
+__device__ __forceinline__ float4 map4(const Map& m, long long i) {
+  return m.p ? __ldg(reinterpret_cast<const float4*>(m.p + i)) : make_float4(m.s, m.s, m.s, m.s);
+}
+__device__ __forceinline__ float4 max4(float4 a, float4 b) {
+  return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+}
+__device__ __forceinline__ float4 min4(float4 a, float4 b) {
+  return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
+}
+__device__ __forceinline__ float2 kahan_add(float2 acc, float v) {
+  const float y = v * v - acc.y;
+  const float t = acc.x + y;
+  acc.y = (t - acc.x) - y;
+  acc.x = t;
+  return acc;
+}
+
+// Dense sensors and full-grid reductions for 4 consecutive points.
+__device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long gi, float4 v) {
+  if (fi <= 0) return;
+  if (s.mode == 1) {
+    if (s.raw) st4(s.raw, (long long)(fi - 1) * s.ns + gi, v);
+    if (s.vmax) st4(s.vmax, gi, fi == 1 ? v : max4(ld4(s.vmax, gi), v));
+    if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
+    if (s.rms) {
+      float4* r = reinterpret_cast<float4*>(s.rms + gi);
+      float4 a = (fi == 1) ? make_float4(0.f, 0.f, 0.f, 0.f) : r[0];
+      float4 b = (fi == 1) ? make_float4(0.f, 0.f, 0.f, 0.f) : r[1];
+      float2 t0 = kahan_add(make_float2(a.x, a.y), v.x), t1 = kahan_add(make_float2(a.z, a.w), v.y);
+      float2 t2 = kahan_add(make_float2(b.x, b.y), v.z), t3 = kahan_add(make_float2(b.z, b.w), v.w);
+      r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
+      r[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+    }
+  }
+  if (s.max_all) st4(s.max_all, gi, fi == 1 ? v : max4(ld4(s.max_all, gi), v));
+  if (s.min_all) st4(s.min_all, gi, fi == 1 ? v : min4(ld4(s.min_all, gi), v));
+}
+
+// Sparse sensors (mode 2) of a row tile, values read from the packed buffer.
+static __device__ void sensor_sparse_tile(const Sensor& s, int fi, const float2* buf, RowLayout lay, const Dims& d,
+                                   long long r0, int L, int* sh) {
+  if (s.mode != 2 || fi <= 0) return;
+  const long long rend = min(r0 + 2LL * L, d.row1);
+  tile_range(s.idx, s.ns, r0 * d.nx, rend * d.nx, sh);
+  const int lo = sh[0], hi = sh[1];
+  for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    const long long local = (long long)__ldg(s.idx + j) - r0 * d.nx;
+    const int q = (int)(local / d.nx), x = (int)(local - (long long)q * d.nx);
+    sensor_put(s, fi, __ldg(s.slot + j), get_comp(buf, lay, q, x));
+  }
+}
+
+__device__ __forceinline__ float src_value(const SparseSource& s, const float* sig, int j, int t) {
+  const int row = (s.nrows_sig == 1) ? 0 : __ldg(s.slot + j);
+  return __ldg(sig + (long long)(t - 1) * s.nrows_sig + row);
+}
+
+template <int NC>
+__device__ __forceinline__ int row_lines(int L) {
+  return NC > 0 ? RTile<NC>::LINES : L;
+}
+
+// ---------------------------------------------------------------------------
+// L2 prefetch of a row tile's inputs.  Issued when the tile starts, so DRAM
+// streams everything the tile will read while the block is still in its
+// first phase; the later loads then hit L2.  Bulk prefetches need 16-byte
+// aligned addresses and sizes: real fields with nx % 4 == 0 and half-spectrum
+// rows rounded up to an even number of bins (the pitch nxp is a multiple of
+// 32 bins, so the rounded row stays inside it).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+struct TilePrefetch {
+  long long r0;
+  int rows;  // rows of the tile inside [row0, row1)
+  int nx;
+  int nxp;
+  int nxh2;  // half-spectrum bins per row, rounded up to even
+  int slot;  // prefetch slots are dealt to the block's threads round robin
+
+  __device__ TilePrefetch(const Dims& d, long long r, int L)
+      : r0(r), rows((int)min(2LL * L, d.row1 - r)), nx(d.nx), nxp(d.nxp), nxh2((d.nxh + 1) & ~1), slot(0) {}
+  __device__ bool mine() { return (int)threadIdx.x == (slot++ % (int)blockDim.x); }
+  // a real field (x fastest): one contiguous range
+  __device__ void field(const void* f, int elem_bytes = 4) {
+    if (!f || rows <= 0) return;
+    if (mine()) prefetch_l2(static_cast<const char*>(f) + r0 * nx * elem_bytes, (unsigned)rows * nx * elem_bytes);
+  }
+  // a half spectrum: one range per row, padding bins skipped
+  __device__ void spectrum(const float2* S) {
+    if (!S) return;
+    for (int t = 0; t < rows; ++t)
+      if (mine()) prefetch_l2(S + (r0 + t) * nxp, (unsigned)nxh2 * 8u);
+  }
+  __device__ void sensor(const Sensor& s, int fi) {
+    if (s.mode != 1 || fi <= 1) return;
+    field(s.vmax);
+    field(s.vmin);
+    field(s.rms, 8);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// u update: C2R of the gradient, split-PML momentum update, velocity
+// sources, velocity sensors, R2C of the new velocity.  blockIdx.y = axis.
+// ---------------------------------------------------------------------------
+template <int NC>
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
+                                                           const __grid_constant__ FFTPlan plan,
+                                                           const float2* __restrict__ tw_g, int Lrt) {
+  extern __shared__ float2 sm[];
+  __shared__ int sh[2];
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
+  const int ax = blockIdx.y;
+  const RowLayout lay{row_layout_stride(nx)};
+  float2* tw = sm;
+  float2* B0 = sm + nx;
+  float2* B1 = CT ? nullptr : B0 + L * lay.ls;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  const int t = *a.clk.t;
+  const int fi = record_index(a.clk);
+  load_c2r<NC>(a.S[ax], B0, lay, d, r0, L, a.kmul[ax]);
+  __syncthreads();
+  if constexpr (NC > 0 && NC % 4 == 0) {  // the epilogue's inputs stream in during the FFT
+    TilePrefetch pf(d, r0, L);
+    if (!a.init) pf.field(a.u[ax]);
+    pf.field(a.rinv[ax].p);
+    pf.sensor(a.sens[ax], fi);
+  }
+  float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
+  float2* W = (G == B0) ? B1 : B0;
+  float* u = a.u[ax];
+  const float* pml = a.pml_sg[ax];
+  const Map rinv = a.rinv[ax];
+  const DenseSource ds = a.dsrc[ax];
+  const bool dense_on = ds.field && t <= ds.len;
+  const float damp = dense_on ? (ds.sig ? __ldg(ds.sig + t - 1) : 1.f) : 0.f;
+  const int total = 2 * L * nx;
+  constexpr bool VEC = NC > 0 && NC % 4 == 0;
+  if constexpr (VEC) {
+    // 4 consecutive points per iteration, 16-byte global accesses
+#pragma unroll 4
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) set_comp(G, lay, q, x + j, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      float4 pm;
+      if (ax == 0) {
+        pm = __ldg(reinterpret_cast<const float4*>(pml + x));
+      } else {
+        const float v = __ldg(pml + (ax == 1 ? (int)(row % d.ny) : (int)(row / d.ny)));
+        pm = make_float4(v, v, v, v);
+      }
+      const float4 rv = map4(rinv, gi);
+      const float4 uo = a.init ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(u, gi);
+      const float4 sv = dense_on ? __ldg(reinterpret_cast<const float4*>(ds.field + gi)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float pmv[4] = {pm.x, pm.y, pm.z, pm.w}, rvv[4] = {rv.x, rv.y, rv.z, rv.w};
+      const float uov[4] = {uo.x, uo.y, uo.z, uo.w}, svv[4] = {sv.x, sv.y, sv.z, sv.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float g = get_comp(G, lay, q, x + j);
+        float un;
+        if (a.init)
+          un = a.dt * rvv[j] * g / 2.f;
+        else
+          un = pmv[j] * (pmv[j] * uov[j] - a.dt * rvv[j] * g);
+        if (dense_on) un = un + damp * svv[j];
+        set_comp(G, lay, q, x + j, un);
+      }
+    }
+  } else {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) {
+        set_comp(G, lay, q, x, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const float g = get_comp(G, lay, q, x);
+      int coord = x;
+      if (ax == 1) coord = (int)(row % d.ny);
+      if (ax == 2) coord = (int)(row / d.ny);
+      const float pm = __ldg(pml + coord);
+      const float rv = rinv.at(gi);
+      float un;
+      if (a.init)
+        un = a.dt * rv * g / 2.f;
+      else
+        un = pm * (pm * u[gi] - a.dt * rv * g);
+      if (dense_on) un = un + damp * __ldg(ds.field + gi);
+      set_comp(G, lay, q, x, un);
+    }
+  }
+  __syncthreads();
+  // sparse velocity sources (dirichlet / additive without correction)
+  const float* ssig = a.src_sig[ax];
+  if (a.src.n > 0 && ssig && t <= a.src_len[ax] && !a.init) {
+    const long long rend = min(r0 + 2LL * L, d.row1);
+    tile_range(a.src.idx, a.src.n, r0 * nx, rend * nx, sh);
+    const int lo = sh[0], hi = sh[1];
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+      const long long local = (long long)__ldg(a.src.idx + j) - r0 * nx;
+      const int q = (int)(local / nx), x = (int)(local - (long long)q * nx);
+      const float v = src_value(a.src, ssig, j, t);
+      const float cur = get_comp(G, lay, q, x);
+      set_comp(G, lay, q, x, a.src.mode == 0 ? v : cur + v);
+    }
+    __syncthreads();
+  }
+  const Sensor& s = a.sens[ax];
+  if constexpr (VEC) {
+#pragma unroll 4
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) continue;
+      const long long gi = row * nx + x;
+      const float4 v = make_float4(get_comp(G, lay, q, x), get_comp(G, lay, q, x + 1), get_comp(G, lay, q, x + 2),
+                                   get_comp(G, lay, q, x + 3));
+      st4(u, gi, v);
+      sensor_dense4(s, fi, gi, v);
+    }
+  } else {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) continue;
+      const long long gi = row * nx + x;
+      const float v = get_comp(G, lay, q, x);
+      u[gi] = v;
+      sensor_dense(s, fi, gi, v);
+    }
+  }
+  sensor_sparse_tile(s, fi, G, lay, d, r0, L, sh);
+  if (a.do_r2c) {
+    __syncthreads();
+    float2* F = tile_fft<NC, false, false>(G, W, tw, plan, L, lay);
+    store_r2c<NC>(F, a.Sout[ax], lay, d, r0, L);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// rho update and equation of state.  C2R of du_i/dx_i for every axis, split
+// mass conservation (linear / nonlinear), pressure sources, then either the
+// lossless / Stokes EOS (p, sensors, R2C of p) or, for power-law absorption,
+// the local part of p plus the R2C of rho0 * sum(du) and sum(rho).
+// ---------------------------------------------------------------------------
+template <int NC, int DIM>
+__global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
+  extern __shared__ float2 sm[];
+  __shared__ int sh[2];
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
+  constexpr int dim = DIM;
+  const RowLayout lay{row_layout_stride(nx)};
+  float2* tw = sm;
+  float2* pool[4];
+  for (int b = 0; b < 4; ++b) pool[b] = sm + nx + b * L * lay.ls;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  const int t = *a.clk.t;
+  const int fi = record_index(a.clk);
+  // inverse x transforms of the divergence components
+  float2* D[3] = {nullptr, nullptr, nullptr};
+  float2* Wk = nullptr;
+  if constexpr (CT) {
+#pragma unroll 1
+    for (int f = 0; f < dim; ++f) {
+      load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L);
+      __syncthreads();
+      if constexpr (NC % 4 == 0) {  // what the next phase reads streams in during this FFT
+        TilePrefetch pf(d, r0, L);
+        if (f + 1 < dim) {
+          pf.spectrum(a.S[f + 1]);
+        } else {
+          _Pragma("unroll") for (int g = 0; g < dim; ++g) pf.field(a.rho[g]);
+          pf.field(a.rho0.p);
+          pf.field(a.c0sq.p);
+          if (a.nonlinear) pf.field(a.bona.p);
+          if (a.eos == 2) pf.field(a.tau.p);
+          if (a.eos != 1) pf.sensor(a.sens, fi);
+        }
+      }
+      tile_fft<NC, true, false>(pool[f], nullptr, tw, plan, L, lay);
+    }
+    _Pragma("unroll") for (int f = 0; f < dim; ++f) D[f] = pool[f];
+  } else {
+    bool used[4] = {false, false, false, false};
+    _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+      int ia = -1, ib = -1;
+      _Pragma("unroll") for (int b = 0; b <= dim; ++b) {
+        if (!used[b]) {
+          if (ia < 0)
+            ia = b;
+          else if (ib < 0)
+            ib = b;
+        }
+      }
+      load_c2r<NC>(a.S[f], pool[ia], lay, d, r0, L);
+      __syncthreads();
+      D[f] = tile_fft<NC, true, false>(pool[ia], pool[ib], tw, plan, L, lay);
+      used[(D[f] == pool[ia]) ? ia : ib] = true;
+    }
+    _Pragma("unroll") for (int b = 0; b <= dim; ++b)
+      if (!used[b]) Wk = pool[b];
+  }
+
+  const bool sp = (a.src.n > 0) && (t <= a.src.len);
+  const bool dense_on = a.dsrc.field && t <= a.dsrc.len;
+  const float damp = dense_on ? (a.dsrc.sig ? __ldg(a.dsrc.sig + t - 1) : 1.f) : 0.f;
+  const int total = 2 * L * nx;
+  const bool absorbing = (a.eos == 1);
+
+  constexpr bool VEC = NC > 0 && NC % 4 == 0;
+  if (VEC && !sp) {
+    // 4 consecutive points per iteration, 16-byte global accesses
+#pragma unroll 2
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x + j, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const int y = (int)(row % d.ny), z = (int)(row / d.ny);
+      float4 ro[3], pm4[3];
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) ro[f] = ld4(a.rho[f], gi);
+      pm4[0] = __ldg(reinterpret_cast<const float4*>(a.pml[0] + x));
+      {
+        const float vy = __ldg(a.pml[1] + y);
+        pm4[1] = make_float4(vy, vy, vy, vy);
+        if (dim == 3) {
+          const float vz = __ldg(a.pml[2] + z);
+          pm4[2] = make_float4(vz, vz, vz, vz);
+        }
+      }
+      const float4 r0v4 = map4(a.rho0, gi);
+      const float4 c24 = map4(a.c0sq, gi);
+      const float4 bn4 = a.nonlinear ? map4(a.bona, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 ta4 = (a.eos == 2) ? map4(a.tau, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 ds4 = dense_on ? __ldg(reinterpret_cast<const float4*>(a.dsrc.field + gi))
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+      float rn[3][4], outp[4], outq[4], outr[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        auto c = [&](const float4& v) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); };
+        float du[3], rold[3];
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+          du[f] = get_comp(D[f], lay, q, x + j);
+          rold[f] = c(ro[f]);
+        }
+        const float r0v = c(r0v4);
+        float rpr = r0v;
+        if (a.nonlinear) {
+          float rs = rold[0] + rold[1];
+          if (dim == 3) rs += rold[2];
+          rpr = 2.f * rs + r0v;
+        }
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+          const float pm = c(pm4[f]);
+          rn[f][j] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
+          if (dense_on) rn[f][j] = rn[f][j] + damp * c(ds4);
+        }
+        float rsum = rn[0][j] + rn[1][j];
+        if (dim == 3) rsum += rn[2][j];
+        float dsum = du[0] + du[1];
+        if (dim == 3) dsum += du[2];
+        float term = rsum;
+        if (a.eos == 2) term = term + c(ta4) * r0v * dsum;
+        if (a.nonlinear) term = term + c(bn4) * rsum * rsum / (2.f * r0v);
+        outp[j] = c(c24) * term;
+        outq[j] = r0v * dsum;
+        outr[j] = rsum;
+      }
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) st4(a.rho[f], gi, make_float4(rn[f][0], rn[f][1], rn[f][2], rn[f][3]));
+      const float4 pv4 = make_float4(outp[0], outp[1], outp[2], outp[3]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (absorbing) {
+          set_comp(D[0], lay, q, x + j, outq[j]);
+          set_comp(D[1], lay, q, x + j, outr[j]);
+        } else {
+          set_comp(D[0], lay, q, x + j, outp[j]);
+        }
+      }
+      if (absorbing) {
+        st4(a.p_loc, gi, pv4);
+      } else {
+        if (a.p_out) st4(a.p_out, gi, pv4);
+        sensor_dense4(a.sens, fi, gi, pv4);
+      }
+    }
+  } else {
+  // Phase A: rho update (stored to global before the EOS when sparse
+  // sources must be applied first).
+  float rnew[3];
+  for (int pass = 0; pass < (sp ? 2 : 1); ++pass) {
+    if (sp && pass == 1) {
+      // apply sparse pressure sources to every rho component in global memory
+      __syncthreads();
+      const long long rend = min(r0 + 2LL * L, d.row1);
+      tile_range(a.src.idx, a.src.n, r0 * nx, rend * nx, sh);
+      const int lo = sh[0], hi = sh[1];
+      for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        const long long gi = __ldg(a.src.idx + j);
+        const float v = src_value(a.src, a.src.sig, j, t);
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) a.rho[f][gi] = (a.src.mode == 0) ? v : a.rho[f][gi] + v;
+      }
+      __syncthreads();
+    }
+#pragma unroll 2
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) {
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) set_comp(D[f], lay, q, x, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      float du[3];
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) du[f] = get_comp(D[f], lay, q, x);
+      const float r0v = a.rho0.at(gi);
+      if (pass == 0) {
+        float rold[3];
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) rold[f] = a.rho[f][gi];
+        float rpr = r0v;
+        if (a.nonlinear) {
+          float rs = rold[0] + rold[1];
+          if (dim == 3) rs += rold[2];
+          rpr = 2.f * rs + r0v;
+        }
+        const int y = (int)(row % d.ny), z = (int)(row / d.ny);
+        const int coord[3] = {x, y, z};
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+          const float pm = __ldg(a.pml[f] + coord[f]);
+          rnew[f] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
+          if (dense_on) rnew[f] = rnew[f] + damp * __ldg(a.dsrc.field + gi);
+          a.rho[f][gi] = rnew[f];
+        }
+        if (sp) continue;
+      } else {
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) rnew[f] = a.rho[f][gi];
+      }
+      // equation of state (kspaceFirstOrder3D.m:963-1017)
+      float rsum = rnew[0] + rnew[1];
+      if (dim == 3) rsum += rnew[2];
+      float dsum = du[0] + du[1];
+      if (dim == 3) dsum += du[2];
+      const float c2 = a.c0sq.at(gi);
+      float term = rsum;
+      if (a.eos == 2) term = term + a.tau.at(gi) * r0v * dsum;
+      if (a.nonlinear) term = term + a.bona.at(gi) * rsum * rsum / (2.f * r0v);
+      const float pv = c2 * term;
+      if (absorbing) {
+        a.p_loc[gi] = pv;
+        set_comp(D[0], lay, q, x, r0v * dsum);
+        set_comp(D[1], lay, q, x, rsum);
+      } else {
+        set_comp(D[0], lay, q, x, pv);
+        if (a.p_out) a.p_out[gi] = pv;
+        sensor_dense(a.sens, fi, gi, pv);
+      }
+    }
+  }
+  }
+  __syncthreads();
+  if (absorbing) {
+    if constexpr (CT) {
+#pragma unroll 1
+      for (int f = 0; f < 2; ++f) {
+        if (f) __syncthreads();
+        tile_fft<NC, false, false>(D[f], nullptr, tw, plan, L, lay);
+        store_r2c<NC>(D[f], f == 0 ? a.S_q : a.S_r, lay, d, r0, L);
+      }
+    } else {
+      float2* F = tile_fft<NC, false, false>(D[0], Wk, tw, plan, L, lay);
+      store_r2c<NC>(F, a.S_q, lay, d, r0, L);
+      __syncthreads();
+      float2* Wk2 = (F == D[0]) ? Wk : D[0];
+      F = tile_fft<NC, false, false>(D[1], Wk2, tw, plan, L, lay);
+      store_r2c<NC>(F, a.S_r, lay, d, r0, L);
+    }
+  } else {
+    sensor_sparse_tile(a.sens, fi, D[0], lay, d, r0, L, sh);
+    __syncthreads();
+    float2* F = tile_fft<NC, false, false>(D[0], Wk, tw, plan, L, lay);
+    store_r2c<NC>(F, a.S_p, lay, d, r0, L);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// power-law absorbing EOS: p = p_loc + c0^2 tau A - c0^2 eta B, sensors, R2C.
+// ---------------------------------------------------------------------------
+template <int NC>
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_constant__ EosArgs a, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
+  extern __shared__ float2 sm[];
+  __shared__ int sh[2];
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
+  const RowLayout lay{row_layout_stride(nx)};
+  float2* tw = sm;
+  float2* P0 = sm + nx;
+  float2* P1 = P0 + L * lay.ls;
+  float2* P2 = CT ? nullptr : P1 + L * lay.ls;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  const int fi = record_index(a.clk);
+  float2 *RA, *RB, *Wk;
+  load_c2r<NC>(a.S_a, P0, lay, d, r0, L);
+  if constexpr (CT) {
+    load_c2r<NC>(a.S_b, P1, lay, d, r0, L);
+    __syncthreads();
+    if constexpr (NC % 4 == 0) {  // the epilogue's inputs stream in during the FFTs
+      TilePrefetch pf(d, r0, L);
+      pf.field(a.p_loc);
+      pf.field(a.c2tau.p);
+      pf.field(a.c2eta.p);
+      pf.sensor(a.sens, fi);
+    }
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) tile_fft<NC, true, false>(f ? P1 : P0, nullptr, tw, plan, L, lay);
+    RA = P0;
+    RB = P1;
+    Wk = nullptr;
+  } else {
+    __syncthreads();
+    RA = tile_fft<NC, true, false>(P0, P1, tw, plan, L, lay);
+    float2* f1 = (RA == P0) ? P1 : P0;
+    load_c2r<NC>(a.S_b, f1, lay, d, r0, L);
+    __syncthreads();
+    RB = tile_fft<NC, true, false>(f1, P2, tw, plan, L, lay);
+    Wk = (RB == f1) ? P2 : f1;
+  }
+  const int total = 2 * L * nx;
+  if constexpr (NC > 0 && NC % 4 == 0) {
+#pragma unroll 4
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) set_comp(RA, lay, q, x + j, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const float4 pl = ld4(a.p_loc, gi), ct = map4(a.c2tau, gi), ce = map4(a.c2eta, gi);
+      const float plv[4] = {pl.x, pl.y, pl.z, pl.w}, ctv[4] = {ct.x, ct.y, ct.z, ct.w};
+      const float cev[4] = {ce.x, ce.y, ce.z, ce.w};
+      float pv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        pv[j] = plv[j] + ctv[j] * get_comp(RA, lay, q, x + j) - cev[j] * get_comp(RB, lay, q, x + j);
+        set_comp(RA, lay, q, x + j, pv[j]);
+      }
+      const float4 p4 = make_float4(pv[0], pv[1], pv[2], pv[3]);
+      if (a.p_out) st4(a.p_out, gi, p4);
+      sensor_dense4(a.sens, fi, gi, p4);
+    }
+  } else {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int q = i / nx, x = i - q * nx;
+      const long long row = r0 + q;
+      if (row >= d.row1) {
+        set_comp(RA, lay, q, x, 0.f);
+        continue;
+      }
+      const long long gi = row * nx + x;
+      const float A = get_comp(RA, lay, q, x);
+      const float B = get_comp(RB, lay, q, x);
+      const float pv = a.p_loc[gi] + a.c2tau.at(gi) * A - a.c2eta.at(gi) * B;
+      set_comp(RA, lay, q, x, pv);
+      if (a.p_out) a.p_out[gi] = pv;
+      sensor_dense(a.sens, fi, gi, pv);
+    }
+  }
+  __syncthreads();
+  sensor_sparse_tile(a.sens, fi, RA, lay, d, r0, L, sh);
+  __syncthreads();
+  float2* F = tile_fft<NC, false, false>(RA, Wk, tw, plan, L, lay);
+  store_r2c<NC>(F, a.S_p, lay, d, r0, L);
+}
+
+// ---------------------------------------------------------------------------
+// plain x transforms (setup work, sources with k-space correction)
+// ---------------------------------------------------------------------------
+template <int NC>
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_r2c(const float* __restrict__ f, float2* S, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
+  extern __shared__ float2 sm[];
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
+  const RowLayout lay{row_layout_stride(nx)};
+  float2* tw = sm;
+  float2* B0 = sm + nx;
+  float2* B1 = CT ? nullptr : B0 + L * lay.ls;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  const int total = 2 * L * nx;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int q = i / nx, x = i - q * nx;
+    const long long row = r0 + q;
+    set_comp(B0, lay, q, x, row < d.row1 ? f[row * nx + x] : 0.f);
+  }
+  __syncthreads();
+  float2* F = tile_fft<NC, false, false>(B0, B1, tw, plan, L, lay);
+  store_r2c<NC>(F, S, lay, d, r0, L);
+}
+
+// out = v (accumulate == 0) or out += v
+template <int NC>
+__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_c2r(const float2* __restrict__ S, float* out,
+                                                             int accumulate, Dims d,
+                                                             const __grid_constant__ FFTPlan plan,
+                                                             const float2* __restrict__ tw_g, int Lrt) {
+  extern __shared__ float2 sm[];
+  constexpr bool CT = NC > 0;
+  const int nx = CT ? NC : d.nx;
+  const int L = row_lines<NC>(Lrt);
+  const RowLayout lay{row_layout_stride(nx)};
+  float2* tw = sm;
+  float2* B0 = sm + nx;
+  float2* B1 = CT ? nullptr : B0 + L * lay.ls;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
+  const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  load_c2r<NC>(S, B0, lay, d, r0, L);
+  __syncthreads();
+  float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
+  const int total = 2 * L * nx;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int q = i / nx, x = i - q * nx;
+    const long long row = r0 + q;
+    if (row >= d.row1) continue;
+    const long long gi = row * nx + x;
+    const float v = get_comp(G, lay, q, x);
+    out[gi] = accumulate ? out[gi] + v : v;
+  }
+}
+
+
+
+// ---------------------------------------------------------------------------
+// host-side launchers of one transform length NC (0: runtime plan).  Each
+// compile-time length is instantiated in a translation unit of its own
+// (generated at build time), so the lengths compile in parallel.
+// ---------------------------------------------------------------------------
+static inline size_t smem_col(int n, int tl, int nbuf) { return sizeof(float2) * ((size_t)n + (size_t)nbuf * tl * n); }
+static inline size_t smem_row(int nx, int L, int nbuf) {
+  return sizeof(float2) * ((size_t)nx + (size_t)nbuf * L * row_layout_stride(nx));
+}
+
+template <class K>
+static inline void set_smem(K k, size_t sm) {
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+}
+
+static inline unsigned row_tiles(const Dims& d, int L) { return (unsigned)((d.row1 - d.row0 + 2 * L - 1) / (2 * L)); }
+
+template <int NC, bool INV>
+static void col_fft_t(const ColArgs& a0, int nfields, long long nouter, const FFTPlan& plan, const float2* tw,
+                      cudaStream_t st) {
+  ColArgs a = a0;
+  const int tl = NC > 0 ? Tile<NC>::LINES : a.tl;
+  a.tl = tl;
+  dim3 grid((a.ncols + tl - 1) / tl, (unsigned)nouter, nfields);
+  const size_t sm = smem_col(plan.n, tl, NC > 0 ? 1 : 2);
+  set_smem(k_col_fft<NC, INV>, sm);
+  k_col_fft<NC, INV><<<grid, Tile<NC>::THREADS, sm, st>>>(a, plan, tw);
+}
+
+template <int NC>
+static void fused_t(const FusedArgs& a0, int ninputs, long long nouter, const FFTPlan& plan, const float2* tw,
+                    const SpecTables& T, int dim, cudaStream_t st) {
+  FusedArgs a = a0;
+  const int tl = NC > 0 ? Tile<NC>::LINES : a.tl;
+  a.tl = tl;
+  dim3 grid((a.ncols + tl - 1) / tl, (unsigned)nouter, ninputs);
+  const size_t sm = smem_col(plan.n, tl, NC > 0 ? 2 : 3);
+  set_smem(k_fused_last<NC>, sm);
+  k_fused_last<NC><<<grid, Tile<NC>::THREADS, sm, st>>>(a, plan, tw, T, dim);
+}
+
+template <int NC>
+static void x_u_t(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt, cudaStream_t st) {
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
+  set_smem(k_x_u<NC>, sm);
+  k_x_u<NC><<<dim3(row_tiles(d, L), d.dim), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+}
+
+template <int NC>
+static void x_rho_t(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
+                    cudaStream_t st) {
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? d.dim : d.dim + 1);
+  if (d.dim == 3) {
+    set_smem(k_x_rho<NC, 3>, sm);
+    k_x_rho<NC, 3><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  } else {
+    set_smem(k_x_rho<NC, 2>, sm);
+    k_x_rho<NC, 2><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  }
+}
+
+template <int NC>
+static void x_eos_t(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
+                    cudaStream_t st) {
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 2 : 3);
+  set_smem(k_x_eos<NC>, sm);
+  k_x_eos<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+}
+
+template <int NC>
+static void x_r2c_t(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt,
+                    cudaStream_t st) {
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
+  set_smem(k_x_r2c<NC>, sm);
+  k_x_r2c<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(f, S, d, plan, tw, L);
+}
+
+template <int NC>
+static void x_c2r_t(const float2* S, float* out, int acc, const Dims& d, const FFTPlan& plan, const float2* tw,
+                    int Lrt, cudaStream_t st) {
+  const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
+  const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
+  set_smem(k_x_c2r<NC>, sm);
+  k_x_c2r<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(S, out, acc, d, plan, tw, L);
+}
+
+// The launchers of one length.  Member functions are defined out of class
+// (so not inline), which lets `extern template` in kernels.cu keep every
+// length out of that translation unit.
+template <int NC>
+struct CtKernels {
+  static void col_fft(bool inv, const ColArgs& a, int nfields, long long nouter, const FFTPlan& plan,
+                      const float2* tw, cudaStream_t st);
+  static void fused(const FusedArgs& a, int ninputs, long long nouter, const FFTPlan& plan, const float2* tw,
+                    const SpecTables& T, int dim, cudaStream_t st);
+  static void x_u(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L, cudaStream_t st);
+  static void x_rho(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                    cudaStream_t st);
+  static void x_eos(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                    cudaStream_t st);
+  static void x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                    cudaStream_t st);
+  static void x_c2r(const float2* S, float* out, int acc, const Dims& d, const FFTPlan& plan, const float2* tw,
+                    int L, cudaStream_t st);
+};
+
+template <int NC>
+void CtKernels<NC>::col_fft(bool inv, const ColArgs& a, int nfields, long long nouter, const FFTPlan& plan,
+                            const float2* tw, cudaStream_t st) {
+  if (inv)
+    col_fft_t<NC, true>(a, nfields, nouter, plan, tw, st);
+  else
+    col_fft_t<NC, false>(a, nfields, nouter, plan, tw, st);
+}
+template <int NC>
+void CtKernels<NC>::fused(const FusedArgs& a, int ninputs, long long nouter, const FFTPlan& plan,
+                          const float2* tw, const SpecTables& T, int dim, cudaStream_t st) {
+  fused_t<NC>(a, ninputs, nouter, plan, tw, T, dim, st);
+}
+template <int NC>
+void CtKernels<NC>::x_u(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                        cudaStream_t st) {
+  x_u_t<NC>(a, d, plan, tw, L, st);
+}
+template <int NC>
+void CtKernels<NC>::x_rho(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                          cudaStream_t st) {
+  x_rho_t<NC>(a, d, plan, tw, L, st);
+}
+template <int NC>
+void CtKernels<NC>::x_eos(const EosArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int L,
+                          cudaStream_t st) {
+  x_eos_t<NC>(a, d, plan, tw, L, st);
+}
+template <int NC>
+void CtKernels<NC>::x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan& plan, const float2* tw,
+                          int L, cudaStream_t st) {
+  x_r2c_t<NC>(f, S, d, plan, tw, L, st);
+}
+template <int NC>
+void CtKernels<NC>::x_c2r(const float2* S, float* out, int acc, const Dims& d, const FFTPlan& plan,
+                          const float2* tw, int L, cudaStream_t st) {
+  x_c2r_t<NC>(S, out, acc, d, plan, tw, L, st);
+}
+
+}  // namespace kwb
+

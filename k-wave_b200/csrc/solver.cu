@@ -949,6 +949,18 @@ void Session::advance(uint64_t n) {
   ck(cudaEventRecord(e, st), "event");
 }
 
+void Session::set_priority(int priority) {
+  int least = 0, greatest = 0;
+  ck(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priority range");
+  priority = std::max(greatest, std::min(least, priority));
+  ck(cudaStreamSynchronize(st), "sync");
+  in_flight();
+  cudaStream_t ns = nullptr;
+  ck(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, priority), "cudaStreamCreateWithPriority");
+  ck(cudaStreamDestroy(st), "cudaStreamDestroy");
+  st = ns;  // the step graph is launched on whatever stream the session holds
+}
+
 uint64_t Session::in_flight() {
   while (!pending_ev.empty()) {
     const cudaError_t q = cudaEventQuery(pending_ev.front());
@@ -1142,6 +1154,21 @@ int kw_session_sync(kw_session* s, kw_status* status) {
 }
 
 uint64_t kw_session_steps_done(const kw_session* s) { return s ? s->s->t_done : 0; }
+
+int kw_stream_priority_range(int* least, int* greatest) {
+  int l = 0, g = 0;
+  const cudaError_t e = cudaDeviceGetStreamPriorityRange(&l, &g);
+  if (least) *least = l;
+  if (greatest) *greatest = g;
+  return e == cudaSuccess ? KW_OK : KW_ERR_CUDA;
+}
+
+int kw_session_set_priority(kw_session* s, int priority, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL session");
+    s->s->set_priority(priority);
+  });
+}
 
 int kw_session_query(kw_session* s, uint64_t* in_flight, kw_status* status) {
   return guarded(status, [&] {

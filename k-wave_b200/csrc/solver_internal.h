@@ -37,6 +37,7 @@ class Session {
   float elapsed_ms();
   void sync();
   uint64_t in_flight();  // advance() calls whose steps have not finished on the device
+  void set_priority(int priority);  // waits for queued work, then re-creates the stream
   void read(kw_output* out);
   uint64_t last_launches_per_step() const { return last_steps ? last_launches / last_steps : 0; }
   static size_t device_bytes_estimate(const kw_input* in, const kw_options* opt);

@@ -93,7 +93,8 @@ EXPORTED = [
     "kw_version", "kw_output_sizes_query", "kw_solve", "kw_run_file", "kw_cli_main",
     "kw_session_create", "kw_session_advance", "kw_session_elapsed_ms", "kw_session_sync",
     "kw_session_steps_done", "kw_session_read", "kw_session_stream", "kw_session_launches_per_step",
-    "kw_session_destroy", "kw_session_query", "kw_kspace_gradient_noalloc",
+    "kw_session_destroy", "kw_session_query", "kw_stream_priority_range", "kw_session_set_priority",
+    "kw_kspace_gradient_noalloc",
 ]
 
 
@@ -117,6 +118,8 @@ def _load():
     lib.kw_session_steps_done.argtypes = [C.c_void_p]
     lib.kw_session_steps_done.restype = C.c_uint64
     lib.kw_session_query.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(KwStatus)]
+    lib.kw_stream_priority_range.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.kw_session_set_priority.argtypes = [C.c_void_p, C.c_int, C.POINTER(KwStatus)]
     lib.kw_session_read.argtypes = [C.c_void_p, C.POINTER(KwOutput), C.POINTER(KwStatus)]
     lib.kw_session_stream.argtypes = [C.c_void_p]
     lib.kw_session_stream.restype = C.c_void_p
@@ -370,6 +373,11 @@ class Session:
     def steps_done(self):
         return int(lib.kw_session_steps_done(self._h))
 
+    def set_priority(self, priority):
+        """CUDA stream priority of the session's work (lower runs first)."""
+        st = KwStatus()
+        _check(lib.kw_session_set_priority(self._h, int(priority), C.byref(st)), st)
+
     def in_flight(self):
         """How many advance() calls still have steps running on the device."""
         st = KwStatus()
@@ -398,6 +406,13 @@ class Session:
 
     def __del__(self):
         self.close()
+
+
+def stream_priority_range():
+    """(least, greatest) CUDA stream priorities of the current device."""
+    lo, hi = C.c_int(0), C.c_int(0)
+    lib.kw_stream_priority_range(C.byref(lo), C.byref(hi))
+    return lo.value, hi.value
 
 
 def kspace_gradient_noalloc(d_f, d_gx, d_gy, nx, ny, dx, dy, c_ref, dt, stream=None):

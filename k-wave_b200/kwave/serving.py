@@ -124,15 +124,22 @@ def library_sizer(r):
 class Server:
     """Admits requests by device-memory budget and interleaves their steps.
 
-    `budget_bytes` bounds the summed estimate of admitted sessions;
-    `chunk` is the number of steps queued per session per call; a session
-    gets its next chunk while fewer than `max_queued` of its chunks are
-    still running, so its stream never runs dry while the host is busy
-    elsewhere.  `clock` / `sleep` are the time source (replaceable by a
-    simulated clock in tests)."""
+    `budget_bytes` bounds the summed estimate of admitted sessions.  Each
+    session is fed chunks of steps (`chunk`, or if 0 about `chunk_seconds`
+    of device time at `step_rate` grid-point-steps/s) while fewer than
+    `max_queued` of its chunks are still running, so its stream never runs
+    dry while the host is busy elsewhere.  With `priorities`, smaller jobs
+    (fewer grid-point-steps) get higher CUDA stream priorities: their
+    kernels are scheduled first and the larger jobs' kernels fill the SMs
+    they leave idle, so short requests are not held up behind long ones.
+    `clock` / `sleep` are the time source (replaceable by a simulated clock
+    in tests)."""
     budget_bytes: int = 150 * 10**9
-    chunk: int = 25
-    max_queued: int = 2
+    chunk: int = 0
+    max_queued: int = 3
+    chunk_seconds: float = 4e-3
+    step_rate: float = 1e10
+    priorities: bool = True
     factory: object = gpu_session
     sizer: object = library_sizer
     clock: object = time.perf_counter
@@ -149,7 +156,8 @@ class Server:
             if r.nbytes > self.budget_bytes:
                 r.error = f"needs {r.nbytes} B of device memory, more than the {self.budget_bytes} B budget"
         queue = [r for r in pending if r.error is None]
-        active = []  # [request, session, steps queued]
+        levels = self._priority_levels() if self.priorities else None
+        active = []  # [request, session, steps queued, chunk]
         used = 0
         t0 = self.clock()
         now = lambda: self.clock() - t0
@@ -163,19 +171,21 @@ class Server:
                 except Exception as e:  # noqa: BLE001 - reported per request
                     r.error = str(e)
                     continue
+                if levels and hasattr(sess, "set_priority"):
+                    sess.set_priority(self._priority(r, levels))
                 r.admitted = now()
                 used += r.nbytes
-                active.append([r, sess, 0])
+                active.append([r, sess, 0, self._chunk(r)])
                 self.log.append(("admit", r.tag, r.admitted, used))
                 progressed = True
             # interleave: top up each session's stream with its next chunk,
             # collect the sessions whose last step has finished
             for a in list(active):
-                r, sess, queued = a
+                r, sess, queued, chunk = a
                 nt = int(r.inp["Nt"])
                 if queued < nt:
                     if sess.in_flight() < self.max_queued:
-                        n = min(self.chunk, nt - queued)
+                        n = min(chunk, nt - queued)
                         sess.advance(n)
                         a[2] = queued + n
                         self.log.append(("advance", r.tag, now(), n))
@@ -195,6 +205,30 @@ class Server:
             if not progressed:
                 self.sleep(self.idle_sleep_s)
         return pending
+
+    def _chunk(self, r):
+        if self.chunk:
+            return self.chunk
+        npts = int(r.inp["Nx"]) * int(r.inp["Ny"]) * int(r.inp["Nz"])
+        return int(max(5, min(200, self.chunk_seconds * self.step_rate / max(npts, 1))))
+
+    @staticmethod
+    def _priority_levels():
+        try:
+            from ._lib import stream_priority_range
+
+            least, greatest = stream_priority_range()
+        except Exception:  # noqa: BLE001 - no device: no priorities
+            return None
+        return list(range(greatest, least + 1))  # highest priority first
+
+    @staticmethod
+    def _priority(r, levels):
+        """One level per decade of grid-point-steps above 1e8."""
+        import math
+
+        k = int(math.log10(max(r.grid_point_steps, 1))) - 8
+        return levels[max(0, min(len(levels) - 1, k))]
 
 
 def serve_plain(requests, factory=gpu_session, clock=time.perf_counter, sleep=time.sleep):

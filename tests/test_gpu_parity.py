@@ -176,3 +176,17 @@ def test_2d_nonlinear_absorbing_512():
     inp, record, start, _ = prepare(kg, medium, {"p0": p0}, {"mask": mask, "record": ["p", "p_rms", "u_max"]},
                                     pml_size=10)
     _check(inp, record, TOL)
+
+
+@pytest.mark.parametrize("n", [(75, 81), (100, 108), (243, 250), (729, 90), (1000, 64), (972, 125)])
+def test_2d_compile_time_mixed_radix_sizes(n):
+    """Compile-time FFT kernels of 2^a 3^b 5^c lengths (radix-3 and -5 stages,
+    line counts that are not multiples of 4, up to 1024 points)."""
+    inp, record, start, _ = case_2d_p0(n=n, nt=30, record=("p", "p_max", "u", "p_final"))
+    _check(inp, record, TOL_LOSSLESS)
+
+
+@pytest.mark.parametrize("n", [(72, 75, 80), (81, 90, 64)])
+def test_3d_compile_time_mixed_radix_sizes(n):
+    inp, record, start, _ = case_3d_het(n=n, nt=24, record=("p", "p_rms", "u"))
+    _check(inp, record, TOL)

@@ -59,7 +59,7 @@ def _server(clock, budget, trace=None, chunk=10):
         return s
 
     srv = serving.Server(budget_bytes=budget, chunk=chunk, factory=factory, sizer=lambda r: r.inp["bytes"],
-                         clock=clock.now, sleep=clock.sleep, idle_sleep_s=1e-4)
+                         priorities=False, clock=clock.now, sleep=clock.sleep, idle_sleep_s=1e-4)
     return srv, made
 
 
@@ -148,3 +148,15 @@ def test_session_bytes_counts_recorded_outputs():
     assert serving.session_bytes(inp, ("u",), Sz) - serving.session_bytes(inp, (), Sz) == 2 * 4 * 10 * 100
     assert serving.session_bytes(inp, ("p_final",), Sz) - serving.session_bytes(inp, (), Sz) == 4 * 1000
     assert base >= 5000
+
+
+def test_priority_levels_follow_job_size_and_chunks_follow_grid_size():
+    levels = [-5, -4, -3, -2, -1, 0]
+    small = serving.Request(inp={"Nx": 256, "Ny": 256, "Nz": 1, "Nt": 500})        # 3.3e7 steps
+    mid = serving.Request(inp={"Nx": 128, "Ny": 128, "Nz": 128, "Nt": 800})        # 1.7e9
+    big = serving.Request(inp={"Nx": 256, "Ny": 256, "Nz": 256, "Nt": 1500})       # 2.5e10
+    p = [serving.Server._priority(r, levels) for r in (small, mid, big)]
+    assert p == [-5, -4, -3] and p == sorted(p)
+    srv = serving.Server(chunk=0, chunk_seconds=4e-3, step_rate=1e10)
+    assert srv._chunk(small) == 200 and srv._chunk(big) == 5
+    assert serving.Server(chunk=17)._chunk(big) == 17
