@@ -30,6 +30,7 @@ enum SpecOpKind {
   OP_SRC_KAPPA = 4,  // cos(c_ref |k| dt / 2)
   OP_IDENTITY = 5,
   OP_KAPPA = 6,      // kappa alone (the axis factor applied elsewhere)
+  OP_SHIFT_NEG = 7,  // exp(-i k_a d_a / 2): staggered -> regular grid along axis a, no kappa
 };
 
 struct SpecOp {
@@ -43,6 +44,7 @@ struct SpecTables {
   const float* k2[3];        // squared wavenumber per axis, FFT order (x: nxh entries)
   const float2* ddk_pos[3];  // i k exp(+i k d / 2), FFT order (x: nxh entries)
   const float2* ddk_neg[3];  // i k exp(-i k d / 2)
+  const float2* shift_neg[3];  // exp(-i k d / 2) (kspaceFirstOrder_createStorageVariables.m)
   float cdt2;                // c_ref * dt / 2
   float ym2, ym1;            // alpha_power - 2, alpha_power - 1
   float scale;               // 1 / (nx ny nz): the inverse-FFT normalisation

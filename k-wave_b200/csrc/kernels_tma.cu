@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
   // per-line tables of the transform axis: shifted derivatives (+, -) and k^2
   float2* dpos = reinterpret_cast<float2*>(bar + 2);
   float2* dneg = dpos + NC;
-  float* kl2 = reinterpret_cast<float*>(dneg + NC);
+  float2* dsh = dneg + NC;
+  float* kl2 = reinterpret_cast<float*>(dsh + NC);
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -131,6 +132,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
     if constexpr (CLS == FC_GRAD) {
       dpos[i] = T.ddk_pos[lax][i];
       dneg[i] = T.ddk_neg[lax][i];
+      dsh[i] = T.shift_neg[lax] ? T.shift_neg[lax][i] : make_float2(1.f, 0.f);
     }
   }
   __syncthreads();
@@ -174,13 +176,17 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
       float2 dconst = make_float2(1.f, 0.f);
       const float2* dline = nullptr;
       float e = 0.f;
+      bool kappa = true;  // the shift operator carries no kappa
       if constexpr (CLS == FC_GRAD) {
         if (op.kind != OP_KAPPA) {
           const bool along = op.axis == lax;
+          kappa = op.kind != OP_SHIFT_NEG;
           if (along) {
-            dline = (op.kind == OP_GRAD_POS) ? dpos : dneg;
+            dline = (op.kind == OP_GRAD_POS) ? dpos : (op.kind == OP_GRAD_NEG ? dneg : dsh);
           } else {
-            const float2* tab = (op.kind == OP_GRAD_POS) ? T.ddk_pos[op.axis] : T.ddk_neg[op.axis];
+            const float2* tab = (op.kind == OP_GRAD_POS)   ? T.ddk_pos[op.axis]
+                                : (op.kind == OP_GRAD_NEG) ? T.ddk_neg[op.axis]
+                                                           : T.shift_neg[op.axis];
             dconst = __ldg(tab + (op.axis == 0 ? ix : o));
           }
         }
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
         const float k2 = kxy2 + kl2[p];
         float m;
         if constexpr (CLS == FC_GRAD) {
-          m = sinc_sq(cdt2sq * k2) * T.scale;
+          m = kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
         } else if constexpr (CLS == FC_NABLA) {
           m = (k2 == 0.f) ? (e == 0.f ? T.scale : 0.f) : exp2f(e * log2f(k2)) * T.scale;
         } else {
@@ -293,7 +299,7 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
 
 template <int NC, int CLS>
 static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
-  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 2 * NC * sizeof(float2) +
+  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
                     NC * sizeof(float);
   auto k = k_fused_tma<NC, CLS>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -308,7 +314,8 @@ static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const Sp
 template <int NC>
 static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   const int kind = a.op[0].kind;
-  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA) return fused_tma_t<NC, FC_GRAD>(a, tw, T, st);
+  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA || kind == OP_SHIFT_NEG)
+    return fused_tma_t<NC, FC_GRAD>(a, tw, T, st);
   if (kind == OP_NABLA1 || kind == OP_NABLA2) return fused_tma_t<NC, FC_NABLA>(a, tw, T, st);
   return fused_tma_t<NC, FC_SRCK>(a, tw, T, st);
 }

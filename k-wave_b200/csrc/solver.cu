@@ -253,18 +253,25 @@ void Session::setup(const kw_input* in, const kw_options* o) {
     std::vector<double> k = kvec_fft_order(ns[a], dd[a]);
     const int cnt = (a == 0) ? d.nxh : ns[a];
     std::vector<float> k2(cnt);
-    std::vector<float2> pos(cnt), neg(cnt);
+    std::vector<float2> pos(cnt), neg(cnt), sh(cnt);
     for (int b = 0; b < cnt; ++b) {
       k2[b] = (float)(k[b] * k[b]);
       std::complex<double> ik(0.0, k[b]);
+      const std::complex<double> e = std::exp(std::complex<double>(0.0, -k[b] * dd[a] / 2));
       std::complex<double> p = ik * std::exp(std::complex<double>(0.0, k[b] * dd[a] / 2));
-      std::complex<double> q = ik * std::exp(std::complex<double>(0.0, -k[b] * dd[a] / 2));
+      std::complex<double> q = ik * e;
       pos[b] = make_float2((float)p.real(), (float)p.imag());
       neg[b] = make_float2((float)q.real(), (float)q.imag());
+      // kspaceFirstOrder_createStorageVariables.m:91-97.  At the Nyquist bin of an
+      // even axis the factor is i; real(ifft(.)) keeps only its Hermitian part,
+      // the real part, which is what a half-spectrum pipeline must apply.
+      const bool nyq = (ns[a] % 2 == 0) && (b == ns[a] / 2);
+      sh[b] = make_float2((float)e.real(), nyq ? 0.f : (float)e.imag());
     }
     T.k2[a] = up(k2_buf[a], k2.data(), cnt, st);
     T.ddk_pos[a] = up(pos_buf[a], pos.data(), cnt, st);
     T.ddk_neg[a] = up(neg_buf[a], neg.data(), cnt, st);
+    T.shift_neg[a] = up(sh_buf[a], sh.data(), cnt, st);
     const uint64_t psz[3] = {in->pml_x_size, in->pml_y_size, in->pml_z_size};
     const double pal[3] = {in->pml_x_alpha, in->pml_y_alpha, in->pml_z_alpha};
     if (psz[a] * 2 > (uint64_t)ns[a]) throw KwError(KW_ERR_INVALID_ARGUMENT, "PML is larger than the grid");
@@ -278,6 +285,7 @@ void Session::setup(const kw_input* in, const kw_options* o) {
     T.k2[2] = T.k2[1];
     T.ddk_pos[2] = T.ddk_pos[1];
     T.ddk_neg[2] = T.ddk_neg[1];
+    T.shift_neg[2] = T.shift_neg[1];
   }
   T.cdt2 = (float)(c_ref * dt / 2.0);
   T.scale = (float)(1.0 / (double)d.npts);
@@ -697,8 +705,30 @@ void Session::setup_sensors(const kw_input* in) {
     const bool any = sens_p.raw || sens_p.vmax || sens_p.vmin || sens_p.rms || sens_p.max_all || sens_p.min_all;
     if (!any) sens_p.mode = 0;
   }
-  if (opt.u_non_staggered_raw)
-    throw KwError(KW_ERR_UNSUPPORTED, "u_non_staggered_raw is not supported yet");
+  if (opt.u_non_staggered_raw && nrec) {
+    for (int a = 0; a < d.dim; ++a) {
+      mk(sens_uns[a]);
+      sens_uns[a].raw = (float*)zalloc(uns_raw_buf[a], ser);
+    }
+    uns_field_buf.alloc(all);
+  }
+}
+
+// u on the regular grid at the sensors (kspaceFirstOrder_extractSensorData.m:109-120):
+// u_a shifted by half a cell back along its own axis,
+// real(ifft(exp(-i k_a d_a / 2) fft(u_a))), one component at a time through S0
+// (free between the gradient and the rho update) and a scratch field.
+void Session::record_non_staggered() {
+  if (!uns_field_buf.p) return;
+  float2* work = (float2*)S_buf[0].p;
+  float* f = (float*)uns_field_buf.p;
+  for (int a = 0; a < d.dim; ++a) {
+    ck(launch_x_r2c((const float*)u_buf[a].p, work, d, plan[0], twd[0], rowL, st), "x_r2c");
+    run_spectral({0}, {0}, {SpecOp{OP_SHIFT_NEG, a}}, 1);
+    ck(launch_x_c2r(work, f, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
+    ck(launch_record_field(f, sens_uns[a], clk, d.npts, st), "record");
+    launches_ += 3;  // r2c, c2r, record (the spectral passes count themselves)
+  }
 }
 
 void Session::build_sensor_lists(const std::vector<uint64_t>& lin, std::vector<int>& si, std::vector<int>& sl) {
@@ -750,6 +780,7 @@ void Session::enqueue_init() {
   ua.do_r2c = 0;
   ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u init");
   ++launches_;
+  record_non_staggered();
   // the x and y transforms of p for the next step's gradient
   ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
   ++launches_;
@@ -848,6 +879,7 @@ void Session::enqueue_step_body(uint64_t t) {
       ++launches_;
       col_pass(false, f123, z0, nzs);
     }
+    record_non_staggered();
     // (2) mass conservation: div u -> rho, EOS (:905-1017)
     {
       std::vector<SpecOp> ops;
@@ -1012,6 +1044,7 @@ void Session::read(kw_output* out) {
   float* uma[3] = {out->ux_max_all, out->uy_max_all, out->uz_max_all};
   float* umi[3] = {out->ux_min_all, out->uy_min_all, out->uz_min_all};
   float* ufi[3] = {out->ux_final, out->uy_final, out->uz_final};
+  float* uns[3] = {out->ux_non_staggered, out->uy_non_staggered, out->uz_non_staggered};
   for (int a = 0; a < d.dim; ++a) {
     d2h(ur[a], u_raw_buf[a].p, ser, st);
     d2h(umx[a], u_max_buf[a].p, per, st);
@@ -1020,6 +1053,7 @@ void Session::read(kw_output* out) {
     d2h(uma[a], u_maxall_buf[a].p, all, st);
     d2h(umi[a], u_minall_buf[a].p, all, st);
     if (opt.u_final) d2h(ufi[a], u_buf[a].p, all, st);
+    d2h(uns[a], uns_raw_buf[a].p, ser, st);
   }
   sync();
 }

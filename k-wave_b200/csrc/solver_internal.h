@@ -92,7 +92,7 @@ class Session {
   uint64_t launches_ = 0, last_launches = 0, last_steps = 0;
 
   // operator tables
-  DevBuf tw_buf[3], k2_buf[3], pos_buf[3], neg_buf[3], pml_buf[3], pmls_buf[3];
+  DevBuf tw_buf[3], k2_buf[3], pos_buf[3], neg_buf[3], sh_buf[3], pml_buf[3], pmls_buf[3];
   const float* pml_d[3]{};
   const float* pml_sg_d[3]{};
   // medium
@@ -122,6 +122,9 @@ class Session {
   const int* sidx_d = nullptr;
   const int* sslot_d = nullptr;
   Sensor sens_p{}, sens_u[3]{};
+  Sensor sens_uns[3]{};                 // u on the regular grid (u_non_staggered_raw)
+  DevBuf uns_raw_buf[3], uns_field_buf;  // its series; the shifted field of one component
+  void record_non_staggered();
   DevBuf p_raw_buf, p_max_buf, p_min_buf, p_rms_buf, p_rmsf_buf, p_maxall_buf, p_minall_buf;
   DevBuf u_raw_buf[3], u_max_buf[3], u_min_buf[3], u_rms_buf[3], u_rmsf_buf[3], u_maxall_buf[3], u_minall_buf[3];
 };

@@ -190,3 +190,41 @@ def test_2d_compile_time_mixed_radix_sizes(n):
 def test_3d_compile_time_mixed_radix_sizes(n):
     inp, record, start, _ = case_3d_het(n=n, nt=24, record=("p", "p_rms", "u"))
     _check(inp, record, TOL)
+
+
+def test_2d_u_non_staggered():
+    """u shifted to the regular grid (kspaceFirstOrder_extractSensorData.m:109-120)."""
+    inp, record, start, _ = case_2d_p0(n=(64, 48), nt=50, record=("p", "u", "u_non_staggered"))
+    gpu = _check(inp, record, TOL_LOSSLESS)
+    assert "ux_non_staggered" in gpu and "uy_non_staggered" in gpu
+    assert not np.allclose(gpu["ux_non_staggered"], gpu["ux"])  # the shift moved the samples
+
+
+@pytest.mark.parametrize("n", [(32, 30, 36), (72, 60, 64), (64, 64, 64)])
+def test_3d_u_non_staggered(n):
+    inp, record, start, _ = case_3d_het(n=n, nt=30, record=("p", "u_non_staggered", "u_rms"))
+    gpu = _check(inp, record, TOL, start=4)
+    assert {"ux_non_staggered", "uy_non_staggered", "uz_non_staggered"} <= set(gpu)
+
+
+def test_intensity_from_the_gpu_path():
+    """sensor.record {'I', 'I_avg'}: p and u_non_staggered from the GPU,
+    intensity on the host (kspaceFirstOrder_saveIntensity.m:42-75), against the
+    same post-processing of the oracle's outputs."""
+    from kwave import _lib
+    from kwave.simulation import postprocess, prepare
+    from kwave.utils import KWaveGrid, make_disc
+
+    n = (64, 64)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    kg.set_time(80, 0.3e-4 / 1500)
+    mask = np.zeros(n)
+    mask[40, 20:44] = 1
+    sensor = {"mask": mask, "record": ["p", "I", "I_avg"]}
+    inp, record, start, meta = prepare(kg, {"sound_speed": 1500.0, "density": 1000.0},
+                                       {"p0": 2 * make_disc(*n, 32, 32, 5)}, sensor, pml_size=8)
+    assert "u_non_staggered" in record
+    gpu = postprocess(_lib.solve(inp, record=record, start_index=start), inp, meta)
+    ora = postprocess(oracle_outputs(inp, record, start, dtype=np.float64), inp, meta)
+    for k in ("Ix", "Iy", "Ix_avg", "Iy_avg"):
+        assert rel_l2(gpu[k], ora[k]) < TOL, k
