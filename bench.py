@@ -168,6 +168,23 @@ def cpu_sample(inp, record, steps=3, warmup=2):
     return npts / per, per
 
 
+def replica_throughput(ms_local, units_local, dist=None, device=None):
+    """Whole-job throughput of independent replicas: the units all ranks
+    processed divided by the slowest rank's time (max over ranks).  Every
+    rank calls it (it is a collective when `dist` is given)."""
+    import torch
+
+    t = torch.tensor([float(ms_local), float(units_local)], dtype=torch.float64, device=device)
+    if dist is not None:
+        ms = t[:1].clone()
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        units = t[1:].clone()
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+        t = torch.cat([ms, units])
+    ms_max, units_all = float(t[0]), float(t[1])
+    return units_all / (ms_max / 1e3), ms_max
+
+
 def batched_sample(n_sims, nt, chunk=25):
     """Config of many independent 3D linear lossy simulations on uneven
     2^a 3^b 5^c grids (64..192 per edge): grid-point-steps/s when they advance
@@ -366,11 +383,7 @@ def main():
     clk = clocks.stop()
     launches_per_step = sess.launches_per_step
     sess.close()
-    ms_t = torch.tensor([ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * npts * args.steps / (ms_max / 1e3)
+    value, ms_max = replica_throughput(ms, npts * args.steps, dist, device="cuda")
     ms_per_step = ms_max / args.steps
 
     # ----- end to end: a whole solve through kw_solve from pinned host memory -----
