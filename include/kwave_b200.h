@@ -176,6 +176,17 @@ int kw_solve(const kw_input* in, const kw_options* opt, kw_output* out, kw_statu
  */
 int kw_run_file(const char* input_h5, const char* output_h5, const kw_options* opt, kw_status* status);
 
+/*
+ * kw_run_file with checkpoints (the binaries' --checkpoint_file,
+ * --checkpoint_timesteps, --checkpoint_interval): the state is written to
+ * `checkpoint_file` every `checkpoint_timesteps` steps and / or every
+ * `checkpoint_interval_s` seconds; if the file exists when the run starts it
+ * is resumed from; it is removed once the output file is written.
+ */
+int kw_run_file_checkpointed(const char* input_h5, const char* output_h5, const kw_options* opt,
+                             const char* checkpoint_file, uint64_t checkpoint_timesteps, double checkpoint_interval_s,
+                             kw_status* status);
+
 /* Command-line entry: the binary's argv, e.g.
  * {"kspaceFirstOrder-B200", "-i", "in.h5", "-o", "out.h5", "--p_raw", "-s", "10"}.
  * Returns the process exit code. */
@@ -209,6 +220,17 @@ int kw_stream_priority_range(int* least, int* greatest);
  * shortest jobs the highest priority: their kernels go first and longer
  * jobs' kernels fill the SMs they leave idle. */
 int kw_session_set_priority(kw_session* s, int priority, kw_status* status);
+/*
+ * Checkpoints (the external binaries' --checkpoint_file; file_type
+ * 'checkpoint', k-Wave/private/getH5Literals.m:48).  kw_session_save waits
+ * for the session's work and writes its state between two steps -- fields,
+ * the pressure spectrum, every sensor accumulator, the step index -- to an
+ * HDF5 file.  kw_session_restore loads such a file into a freshly created
+ * session of the same input and options; the run then continues bit for bit
+ * as if it had never stopped.
+ */
+int kw_session_save(kw_session* s, const char* path, kw_status* status);
+int kw_session_restore(kw_session* s, const char* path, kw_status* status);
 /* Copy the outputs recorded so far into host buffers. */
 int kw_session_read(kw_session* s, kw_output* out, kw_status* status);
 /* The session's CUDA stream (a cudaStream_t), for event timing by callers. */

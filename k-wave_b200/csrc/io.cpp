@@ -3,6 +3,8 @@
 // solver, and write the output file that k-Wave/kspaceFirstOrder3DC.m:569-776
 // reads back.  kw_cli_main() parses the command line those wrappers build
 // (kspaceFirstOrder3DC.m:462-545).
+#include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -169,6 +171,41 @@ void read_input(const std::string& path, InputFile& F) {
   }
 }
 
+// Solve with checkpoints: a resident session advanced in chunks, its state
+// written to `ckpt` every `every_steps` steps and / or `every_s` seconds of
+// wall time; an existing checkpoint file is resumed from.
+void solve_checkpointed(const kw_input& in, const kw_options& opt, kw_output& out, const char* ckpt,
+                        uint64_t every_steps, double every_s) {
+  kw_session* s = nullptr;
+  kw_status e{};
+  if (kw_session_create(&in, &opt, &s, &e) != KW_OK) throw IoError(e.code, e.message);
+  struct Guard {
+    kw_session* s;
+    ~Guard() { kw_session_destroy(s); }
+  } guard{s};
+  if (FILE* f = std::fopen(ckpt, "rb")) {
+    std::fclose(f);
+    if (kw_session_restore(s, ckpt, &e) != KW_OK) throw IoError(e.code, e.message);
+  }
+  const uint64_t chunk = every_steps ? every_steps : 50;
+  uint64_t done = kw_session_steps_done(s), since = 0;
+  auto last = std::chrono::steady_clock::now();
+  while (done < in.Nt) {
+    const uint64_t n = std::min<uint64_t>(chunk - since % chunk, in.Nt - done);
+    if (kw_session_advance(s, n, &e) != KW_OK || kw_session_sync(s, &e) != KW_OK) throw IoError(e.code, e.message);
+    done += n;
+    since += n;
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - last).count();
+    const bool due = (every_steps && since >= every_steps) || (every_s > 0 && el >= every_s);
+    if (due && done < in.Nt) {
+      if (kw_session_save(s, ckpt, &e) != KW_OK) throw IoError(e.code, e.message);
+      since = 0;
+      last = std::chrono::steady_clock::now();
+    }
+  }
+  if (kw_session_read(s, &out, &e) != KW_OK) throw IoError(e.code, e.message);
+}
+
 std::string now_string() {
   char buf[64];
   std::time_t t = std::time(nullptr);
@@ -178,7 +215,8 @@ std::string now_string() {
 
 }  // namespace
 
-extern "C" int kw_run_file(const char* input_h5, const char* output_h5, const kw_options* opt_in, kw_status* st) {
+static int run_file(const char* input_h5, const char* output_h5, const kw_options* opt_in, const char* ckpt,
+                    uint64_t ckpt_steps, double ckpt_s, kw_status* st) {
   try {
     if (!input_h5 || !output_h5 || !opt_in) throw IoError(KW_ERR_INVALID_ARGUMENT, "NULL argument");
     kw_options opt = *opt_in;
@@ -227,8 +265,12 @@ extern "C" int kw_run_file(const char* input_h5, const char* output_h5, const kw
       if (opt.u_final) buf(u_fin[a], ng);
       if (opt.u_non_staggered_raw) buf(u_nst[a], ns * nr);
     }
-    kw_status s3{};
-    if (kw_solve(&F.in, &opt, &out, &s3) != KW_OK) throw IoError(s3.code, s3.message);
+    if (ckpt) {
+      solve_checkpointed(F.in, opt, out, ckpt, ckpt_steps, ckpt_s);
+    } else {
+      kw_status s3{};
+      if (kw_solve(&F.in, &opt, &out, &s3) != KW_OK) throw IoError(s3.code, s3.message);
+    }
 
     // output file (kspaceFirstOrder3DC.m:569-776)
     h5::Writer w;
@@ -324,6 +366,7 @@ extern "C" int kw_run_file(const char* input_h5, const char* output_h5, const kw
     } catch (const h5::Error& e) {
       throw IoError(KW_ERR_IO, e.what());
     }
+    if (ckpt) std::remove(ckpt);  // the run is complete: the checkpoint is spent
     return set_status(st, KW_OK, "");
   } catch (const IoError& e) {
     return set_status(st, e.code, e.what());
@@ -334,11 +377,25 @@ extern "C" int kw_run_file(const char* input_h5, const char* output_h5, const kw
   }
 }
 
+extern "C" int kw_run_file(const char* input_h5, const char* output_h5, const kw_options* opt, kw_status* st) {
+  return run_file(input_h5, output_h5, opt, nullptr, 0, 0.0, st);
+}
+
+extern "C" int kw_run_file_checkpointed(const char* input_h5, const char* output_h5, const kw_options* opt,
+                                        const char* checkpoint_file, uint64_t checkpoint_timesteps,
+                                        double checkpoint_interval_s, kw_status* st) {
+  if (!checkpoint_file || (!checkpoint_timesteps && !(checkpoint_interval_s > 0)))
+    return set_status(st, KW_ERR_INVALID_ARGUMENT, "a checkpoint file and an interval (steps or seconds) are needed");
+  return run_file(input_h5, output_h5, opt, checkpoint_file, checkpoint_timesteps, checkpoint_interval_s, st);
+}
+
 // kspaceFirstOrder-B200 -i in.h5 -o out.h5 [--p_raw] [--p_max] ... [-s N] [-g N]
 extern "C" int kw_cli_main(int argc, char** argv) {
   kw_options opt{};
   opt.device = -1;
-  std::string in, out;
+  std::string in, out, ckpt;
+  uint64_t ckpt_steps = 0;
+  double ckpt_s = 0.0;
   bool any = false;
   struct Flag {
     const char* name;
@@ -354,7 +411,8 @@ extern "C" int kw_cli_main(int argc, char** argv) {
     std::fprintf(stderr,
                  "usage: %s -i <input.h5> -o <output.h5> [--p_raw --p_max --p_min --p_rms --p_max_all --p_min_all "
                  "--p_final --u_raw --u_max --u_min --u_rms --u_max_all --u_min_all --u_final "
-                 "--u_non_staggered_raw] [-s <start index>] [-g <device>] [-t <threads>] [--verbose <0-2>]\n",
+                 "--u_non_staggered_raw] [-s <start index>] [-g <device>] [-t <threads>] [--verbose <0-2>] "
+                 "[--checkpoint_file <file> --checkpoint_timesteps <n> | --checkpoint_interval <seconds>]\n",
                  prog);
     return 2;
   };
@@ -392,6 +450,18 @@ extern "C" int kw_cli_main(int argc, char** argv) {
       const char* v = value();
       if (!v) return usage();
       opt.verbose = std::atoi(v);
+    } else if (a == "--checkpoint_file") {
+      const char* v = value();
+      if (!v) return usage();
+      ckpt = v;
+    } else if (a == "--checkpoint_timesteps") {
+      const char* v = value();
+      if (!v) return usage();
+      ckpt_steps = std::strtoull(v, nullptr, 10);
+    } else if (a == "--checkpoint_interval") {
+      const char* v = value();
+      if (!v) return usage();
+      ckpt_s = std::atof(v);
     } else if (a == "-t" || a == "-c" || a == "--benchmark") {
       if (!value()) return usage();  // host threads / compression level: not used by the GPU solver
     } else if (a == "-h" || a == "--help") {
@@ -406,7 +476,13 @@ extern "C" int kw_cli_main(int argc, char** argv) {
   if (!any) opt.p_raw = 1;  // the binaries record p when no output is named
   kw_status st{};
   if (opt.verbose) std::printf("%s: %s -> %s\n", kw_version(), in.c_str(), out.c_str());
-  const int rc = kw_run_file(in.c_str(), out.c_str(), &opt, &st);
+  if (!ckpt.empty() && !ckpt_steps && !(ckpt_s > 0)) {
+    std::fprintf(stderr, "%s: --checkpoint_file needs --checkpoint_timesteps or --checkpoint_interval\n", prog);
+    return usage();
+  }
+  const int rc = ckpt.empty() ? kw_run_file(in.c_str(), out.c_str(), &opt, &st)
+                              : kw_run_file_checkpointed(in.c_str(), out.c_str(), &opt, ckpt.c_str(), ckpt_steps,
+                                                         ckpt_s, &st);
   if (rc != KW_OK) {
     std::fprintf(stderr, "%s: error %d: %s\n", prog, rc, st.message);
     return 1;

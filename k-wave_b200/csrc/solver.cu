@@ -24,6 +24,7 @@
 
 #include "kernels.cuh"
 #include "kwave_b200.h"
+#include "hdf5_lite.h"
 #include "solver_internal.h"
 
 namespace kwb {
@@ -993,6 +994,97 @@ void Session::set_priority(int priority) {
   st = ns;  // the step graph is launched on whatever stream the session holds
 }
 
+// Everything a step reads from the previous one: the split densities, the
+// staggered velocities, the pressure spectrum S0 (p transformed along x and
+// y, raw), and every sensor accumulator.  Source fields, medium maps and
+// operator tables are rebuilt from the input by setup().
+std::vector<std::pair<std::string, DevBuf*>> Session::state_buffers() {
+  std::vector<std::pair<std::string, DevBuf*>> v;
+  const char* c = "xyz";
+  for (int a = 0; a < d.dim; ++a) {
+    v.push_back({std::string("rho_") + c[a], &rho_buf[a]});
+    v.push_back({std::string("u_") + c[a] + "_sg", &u_buf[a]});
+  }
+  v.push_back({"p_spectrum", &S_buf[0]});
+  v.push_back({"p", &p_raw_buf});
+  v.push_back({"p_max", &p_max_buf});
+  v.push_back({"p_min", &p_min_buf});
+  v.push_back({"p_rms_acc", &p_rms_buf});
+  v.push_back({"p_max_all", &p_maxall_buf});
+  v.push_back({"p_min_all", &p_minall_buf});
+  for (int a = 0; a < d.dim; ++a) {
+    const std::string u = std::string("u") + c[a];
+    v.push_back({u, &u_raw_buf[a]});
+    v.push_back({u + "_max", &u_max_buf[a]});
+    v.push_back({u + "_min", &u_min_buf[a]});
+    v.push_back({u + "_rms_acc", &u_rms_buf[a]});
+    v.push_back({u + "_max_all", &u_maxall_buf[a]});
+    v.push_back({u + "_min_all", &u_minall_buf[a]});
+    v.push_back({u + "_non_staggered", &uns_raw_buf[a]});
+  }
+  return v;
+}
+
+void Session::save_checkpoint(const std::string& path) {
+  sync();
+  h5::Writer w;
+  std::vector<std::vector<float>> host;
+  host.reserve(64);
+  for (auto& nb : state_buffers()) {
+    DevBuf* b = nb.second;
+    if (!b->p || !b->bytes) continue;
+    host.emplace_back(b->bytes / sizeof(float));
+    ck(cudaMemcpy(host.back().data(), b->p, b->bytes, cudaMemcpyDeviceToHost), "checkpoint d2h");
+    w.dataset("/" + nb.first, h5::DType::F32, {(uint64_t)host.back().size()}, host.back().data());
+  }
+  const uint64_t meta[5] = {t_done, (uint64_t)d.nx, (uint64_t)d.ny, (uint64_t)d.nz, Nt};
+  const char* names[5] = {"t_index", "Nx", "Ny", "Nz", "Nt"};
+  for (int i = 0; i < 5; ++i) w.dataset(std::string("/") + names[i], h5::DType::U64, {1}, &meta[i]);
+  w.root_attribute("created_by", kw_version());
+  w.root_attribute("file_type", "checkpoint");
+  w.root_attribute("major_version", "1");
+  w.root_attribute("minor_version", "2");
+  try {
+    w.write(path);
+  } catch (const h5::Error& e) {
+    throw KwError(KW_ERR_IO, e.what());
+  }
+}
+
+void Session::restore_checkpoint(const std::string& path) {
+  if (t_done != 0) throw KwError(KW_ERR_INVALID_ARGUMENT, "a checkpoint is restored into a fresh session only");
+  try {
+    h5::Reader r(path);
+    if (r.attribute_string("/", "file_type") != "checkpoint")
+      throw KwError(KW_ERR_IO, path + " is not a checkpoint file");
+    auto one = [&](const char* n) -> uint64_t {
+      auto v = r.read_u64(std::string("/") + n);
+      if (v.size() != 1) throw KwError(KW_ERR_IO, std::string("checkpoint lacks ") + n);
+      return v[0];
+    };
+    if (one("Nx") != (uint64_t)d.nx || one("Ny") != (uint64_t)d.ny || one("Nz") != (uint64_t)d.nz ||
+        one("Nt") != Nt)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "the checkpoint belongs to a different simulation");
+    const uint64_t t = one("t_index");
+    if (t > Nt) throw KwError(KW_ERR_IO, "checkpoint time index beyond Nt");
+    for (auto& nb : state_buffers()) {
+      DevBuf* b = nb.second;
+      if (!b->p || !b->bytes) continue;
+      const std::string name = "/" + nb.first;
+      if (!r.exists(name))
+        throw KwError(KW_ERR_INVALID_ARGUMENT, "checkpoint lacks " + nb.first + " (recorded outputs differ)");
+      std::vector<float> v = r.read_float(name);
+      if (v.size() * sizeof(float) != b->bytes) throw KwError(KW_ERR_IO, "checkpoint dataset size of " + nb.first);
+      ck(cudaMemcpy(b->p, v.data(), b->bytes, cudaMemcpyHostToDevice), "checkpoint h2d");
+    }
+    t_done = t;
+    const int clock = (int)t + 1;  // the device clock holds the index of the next step
+    ck(cudaMemcpy(clock_buf.p, &clock, sizeof(int), cudaMemcpyHostToDevice), "clock");
+  } catch (const h5::Error& e) {
+    throw KwError(KW_ERR_IO, path + ": " + e.what());
+  }
+}
+
 uint64_t Session::in_flight() {
   while (!pending_ev.empty()) {
     const cudaError_t q = cudaEventQuery(pending_ev.front());
@@ -1195,6 +1287,20 @@ int kw_stream_priority_range(int* least, int* greatest) {
   if (least) *least = l;
   if (greatest) *greatest = g;
   return e == cudaSuccess ? KW_OK : KW_ERR_CUDA;
+}
+
+int kw_session_save(kw_session* s, const char* path, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s || !path) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL argument");
+    s->s->save_checkpoint(path);
+  });
+}
+
+int kw_session_restore(kw_session* s, const char* path, kw_status* status) {
+  return guarded(status, [&] {
+    if (!s || !path) throw KwError(KW_ERR_INVALID_ARGUMENT, "NULL argument");
+    s->s->restore_checkpoint(path);
+  });
 }
 
 int kw_session_set_priority(kw_session* s, int priority, kw_status* status) {

@@ -5,6 +5,7 @@
 #include <deque>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "kernels.cuh"
@@ -37,6 +38,10 @@ class Session {
   float elapsed_ms();
   void sync();
   uint64_t in_flight();  // advance() calls whose steps have not finished on the device
+  // checkpoints: the state between two steps, written to / read from an HDF5 file
+  void save_checkpoint(const std::string& path);
+  void restore_checkpoint(const std::string& path);
+  std::vector<std::pair<std::string, DevBuf*>> state_buffers();
   void set_priority(int priority);  // waits for queued work, then re-creates the stream
   void read(kw_output* out);
   uint64_t last_launches_per_step() const { return last_steps ? last_launches / last_steps : 0; }

@@ -90,10 +90,11 @@ class KwOutputSizes(C.Structure):
 
 
 EXPORTED = [
-    "kw_version", "kw_output_sizes_query", "kw_solve", "kw_run_file", "kw_cli_main",
+    "kw_version", "kw_output_sizes_query", "kw_solve", "kw_run_file", "kw_run_file_checkpointed", "kw_cli_main",
     "kw_session_create", "kw_session_advance", "kw_session_elapsed_ms", "kw_session_sync",
     "kw_session_steps_done", "kw_session_read", "kw_session_stream", "kw_session_launches_per_step",
     "kw_session_destroy", "kw_session_query", "kw_stream_priority_range", "kw_session_set_priority",
+    "kw_session_save", "kw_session_restore",
     "kw_kspace_gradient_noalloc",
 ]
 
@@ -110,6 +111,8 @@ def _load():
                              C.POINTER(KwStatus)]
     lib.kw_run_file.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(KwOptions), C.POINTER(KwStatus)]
     lib.kw_cli_main.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
+    lib.kw_run_file_checkpointed.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(KwOptions), C.c_char_p, C.c_uint64,
+                                             C.c_double, C.POINTER(KwStatus)]
     lib.kw_session_create.argtypes = [C.POINTER(KwInput), C.POINTER(KwOptions), C.POINTER(C.c_void_p),
                                       C.POINTER(KwStatus)]
     lib.kw_session_advance.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(KwStatus)]
@@ -120,6 +123,8 @@ def _load():
     lib.kw_session_query.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(KwStatus)]
     lib.kw_stream_priority_range.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.kw_session_set_priority.argtypes = [C.c_void_p, C.c_int, C.POINTER(KwStatus)]
+    lib.kw_session_save.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(KwStatus)]
+    lib.kw_session_restore.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(KwStatus)]
     lib.kw_session_read.argtypes = [C.c_void_p, C.POINTER(KwOutput), C.POINTER(KwStatus)]
     lib.kw_session_stream.argtypes = [C.c_void_p]
     lib.kw_session_stream.restype = C.c_void_p
@@ -326,12 +331,20 @@ def solve(inp: dict, record=("p",), start_index=1, device=-1):
     return to_matlab_layout(bufs, inp)
 
 
-def run_file(input_path, output_path, record=("p",), start_index=1, device=-1, verbose=0):
+def run_file(input_path, output_path, record=("p",), start_index=1, device=-1, verbose=0, checkpoint=None,
+             checkpoint_timesteps=0, checkpoint_interval=0.0):
     """kw_run_file(): read a k-Wave HDF5 input file, run it, write the output
-    file (what kspaceFirstOrder3DC.m:560-567 does through the binary)."""
+    file (what kspaceFirstOrder3DC.m:560-567 does through the binary).  With
+    `checkpoint`, the state is saved there every `checkpoint_timesteps` steps
+    and / or `checkpoint_interval` seconds and resumed from if it exists."""
     opt = make_options(record, start_index, device, verbose)
     st = KwStatus()
-    _check(lib.kw_run_file(os.fsencode(input_path), os.fsencode(output_path), C.byref(opt), C.byref(st)), st)
+    if checkpoint is None:
+        _check(lib.kw_run_file(os.fsencode(input_path), os.fsencode(output_path), C.byref(opt), C.byref(st)), st)
+    else:
+        _check(lib.kw_run_file_checkpointed(os.fsencode(input_path), os.fsencode(output_path), C.byref(opt),
+                                            os.fsencode(checkpoint), int(checkpoint_timesteps),
+                                            float(checkpoint_interval), C.byref(st)), st)
 
 
 def cli_main(argv):
@@ -372,6 +385,16 @@ class Session:
     @property
     def steps_done(self):
         return int(lib.kw_session_steps_done(self._h))
+
+    def save(self, path):
+        """Write a checkpoint of the state between two steps (waits for queued work)."""
+        st = KwStatus()
+        _check(lib.kw_session_save(self._h, os.fsencode(path), C.byref(st)), st)
+
+    def restore(self, path):
+        """Continue from a checkpoint (this session must be fresh, same input and options)."""
+        st = KwStatus()
+        _check(lib.kw_session_restore(self._h, os.fsencode(path), C.byref(st)), st)
 
     def set_priority(self, priority):
         """CUDA stream priority of the session's work (lower runs first)."""

@@ -284,5 +284,6 @@ def test_command_line(tmp_path):
     assert run("-i", "x.h5", "-o").returncode == 2
     r = run("-i", str(tmp_path / "missing.h5"), "-o", str(tmp_path / "o.h5"), "--p_max", "-t", "8")
     assert r.returncode == 1 and "missing.h5" in r.stderr
+    assert run("-i", "x.h5", "-o", "y.h5", "--checkpoint_file", "c.h5").returncode == 2  # needs an interval
     assert _lib.cli_main(["prog", "--help"]) == 0
     assert _lib.cli_main(["prog", "-i"]) == 2
