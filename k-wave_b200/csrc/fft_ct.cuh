@@ -159,6 +159,69 @@ __device__ __forceinline__ void ct_stages(float2* buf, const float2* __restrict_
   }
 }
 
+// Register hand-off between a forward transform and an inverse one of the
+// same line.  Thread `tid` of a line owns positions tid + T*m, m < N/T, in
+// two places: they are the outputs of its butterflies in the last stage
+// (position j + r*NS, NS = N / R_last, j = tid + i*T) and the inputs of its
+// butterflies in the first stage (position j + r*N/R_0), provided T divides
+// N / R_last and N / R_0 (the largest radix is a multiple of the first and
+// last ones: 64 = 16*4, 128 = 16*8, 256 = 16*16).  A spectral operator can
+// then be applied in registers between the forward transform's last stage
+// and the inverse transform's first, without a shared-memory round trip.
+template <int N>
+struct CtHandoff {
+  static constexpr int S = Ct<N>::S;
+  static constexpr int T = Ct<N>::T;
+  static constexpr int M = N / T;  // positions per thread
+  static constexpr bool OK = S >= 2 && (ct_ns(N, S - 1) % T == 0) && ((N / ct_radix(N, 0)) % T == 0);
+};
+
+// Forward last stage of line `l` read from `src`; u[m] receives position tid + T*m.
+template <int N, class L>
+__device__ __forceinline__ void ct_fwd_last_to_regs(const float2* __restrict__ src, const float2* __restrict__ tw,
+                                                    int l, int tid, L lay, float2 (&u)[CtHandoff<N>::M]) {
+  static_assert(CtHandoff<N>::OK, "no register hand-off for this plan");
+  constexpr int STAGE = Ct<N>::S - 1;
+  constexpr int R = ct_radix(N, STAGE);
+  constexpr int NS = ct_ns(N, STAGE);  // = N / R: the stride of the outputs
+  constexpr int NR = N / R;
+  constexpr int T = Ct<N>::T;
+  constexpr int TWS = N / (NS * R);
+#pragma unroll
+  for (int i = 0; i < NR / T; ++i) {
+    const int j = tid + i * T;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[lay(l, j + r * NR)];
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], tw[j * r * TWS]);  // k = j % NS = j
+    dft<R, false>(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) u[i + r * (NS / T)] = v[r];  // position j + r * NS
+  }
+}
+
+// Inverse first stage from registers (u[m] = position tid + T*m); stores its
+// outputs to `dst` in the order the next stage reads (as ct_stage does).
+template <int N, class L>
+__device__ __forceinline__ void ct_inv_first_from_regs(const float2 (&u)[CtHandoff<N>::M], float2* __restrict__ dst,
+                                                       int l, int tid, L lay) {
+  static_assert(CtHandoff<N>::OK, "no register hand-off for this plan");
+  constexpr int R = ct_radix(N, 0);
+  constexpr int NR = N / R;
+  constexpr int T = Ct<N>::T;
+#pragma unroll
+  for (int i = 0; i < NR / T; ++i) {
+    const int j = tid + i * T;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = u[i + r * (NR / T)];  // position j + r * NR
+    dft<R, true>(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[lay(l, j * R + r)] = v[r];
+  }
+}
+
 // In-place transform of LINES lines by T * LINES threads.  LINE_FAST maps
 // consecutive threads to consecutive lines (column tiles, whose lines are
 // adjacent in shared memory); otherwise to consecutive butterflies of one

@@ -102,7 +102,9 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
 // only that operator's arithmetic in the kernel body.
 enum FusedClass { FC_GRAD = 0, FC_NABLA = 1, FC_SRCK = 2 };
 
-template <int NC, int CLS>
+// ONE: every input has a single output (the register hand-off path);
+// otherwise the forward transform is kept and each output multiplied from it.
+template <int NC, int CLS, bool ONE>
 __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
                                                                      const float2* __restrict__ tw_g,
                                                                      const __grid_constant__ SpecTables T) {
@@ -159,6 +161,9 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
   // the line mapping fixes this thread's column (kx) for every pass
   const int l = threadIdx.x % TL, tid = threadIdx.x / TL;
   const float cdt2sq = T.cdt2 * T.cdt2;
+  constexpr int TPL = TH / TL;  // threads per line
+  constexpr int M = CtHandoff<NC>::M;
+  static_assert(TPL == Ct<NC>::T, "one line per group of T threads");
   int it = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -168,53 +173,56 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
     const int x0 = cx * TL;
     const int ix = min(x0 + l, a.ncols - 1);
     const float kxy2 = __ldg(T.k2[0] + ix) + ((a.dim == 3) ? __ldg(T.k2[1] + o) : 0.f);
-    mbar_wait(&bar[s], (it >> 1) & 1, a.err);
-    ct_fft<NC, false, true, TL>(F, tw, lay);
-#pragma unroll 1
-    for (int q = 0; q < a.fanout; ++q) {
+    // the operator of output q: a real factor m(|k|^2), times a complex
+    // factor that is constant along the line or read from a line table
+    struct OpEval {
+      float2 dconst;
+      const float2* dline;
+      float e;
+      bool kappa;
+    };
+    auto setup = [&](int q) {
       const SpecOp op = a.op[g * a.fanout + q];
-      float2 dconst = make_float2(1.f, 0.f);
-      const float2* dline = nullptr;
-      float e = 0.f;
-      bool kappa = true;  // the shift operator carries no kappa
+      OpEval ev{make_float2(1.f, 0.f), nullptr, 0.f, true};
       if constexpr (CLS == FC_GRAD) {
         if (op.kind != OP_KAPPA) {
-          const bool along = op.axis == lax;
-          kappa = op.kind != OP_SHIFT_NEG;
-          if (along) {
-            dline = (op.kind == OP_GRAD_POS) ? dpos : (op.kind == OP_GRAD_NEG ? dneg : dsh);
+          ev.kappa = op.kind != OP_SHIFT_NEG;  // the shift operator carries no kappa
+          if (op.axis == lax) {
+            ev.dline = (op.kind == OP_GRAD_POS) ? dpos : (op.kind == OP_GRAD_NEG ? dneg : dsh);
           } else {
             const float2* tab = (op.kind == OP_GRAD_POS)   ? T.ddk_pos[op.axis]
                                 : (op.kind == OP_GRAD_NEG) ? T.ddk_neg[op.axis]
                                                            : T.shift_neg[op.axis];
-            dconst = __ldg(tab + (op.axis == 0 ? ix : o));
+            ev.dconst = __ldg(tab + (op.axis == 0 ? ix : o));
           }
         }
       } else if constexpr (CLS == FC_NABLA) {
-        e = 0.5f * ((op.kind == OP_NABLA1) ? T.ym2 : T.ym1);  // |k|^y = (|k|^2)^(y/2)
+        ev.e = 0.5f * ((op.kind == OP_NABLA1) ? T.ym2 : T.ym1);  // |k|^y = (|k|^2)^(y/2)
       }
-      // W = F * operator (one pass; positions p = tid + k * (TH / TL))
-#pragma unroll 4
-      for (int p = tid; p < NC; p += TH / TL) {
+      return ev;
+    };
+    auto apply = [&](const OpEval& ev, float2 (&u)[M]) {
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int p = tid + TPL * m;
         const float k2 = kxy2 + kl2[p];
-        float m;
+        float f;
         if constexpr (CLS == FC_GRAD) {
-          m = kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
+          f = ev.kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
+          u[m] = c_mul(c_scale(u[m], f), ev.dline ? ev.dline[p] : ev.dconst);
         } else if constexpr (CLS == FC_NABLA) {
-          m = (k2 == 0.f) ? (e == 0.f ? T.scale : 0.f) : exp2f(e * log2f(k2)) * T.scale;
+          f = (k2 == 0.f) ? (ev.e == 0.f ? T.scale : 0.f) : exp2f(ev.e * log2f(k2)) * T.scale;
+          u[m] = c_scale(u[m], f);
         } else {
-          m = cos_sq(cdt2sq * k2) * T.scale;
+          f = cos_sq(cdt2sq * k2) * T.scale;
+          u[m] = c_scale(u[m], f);
         }
-        float2 f = F[lay(l, p)];
-        f = make_float2(f.x * m, f.y * m);
-        if constexpr (CLS == FC_GRAD) f = c_mul(f, dline ? dline[p] : dconst);
-        W[lay(l, p)] = f;
       }
-      __syncthreads();
-      // inverse: stage 0 in place, stage 1 straight to the output buffer
-      ct_stage<NC, 0, true>(W, tw, l, tid, lay);
+    };
+    // inverse last stage, straight from W to the output (and the optional
+    // second output scaled by a factor constant along the line)
+    auto finish = [&](int q) {
       float2* dst = a.outp[g * a.fanout + q] + (long long)o * a.ostride + x0;
-      // optional second output scaled by a factor constant along the line
       float2* dst2 = a.dual_outp[g * a.fanout + q];
       float2 dsc = make_float2(0.f, 0.f);
       if (dst2) {
@@ -230,14 +238,55 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
         }
       };
       ct_stage_io<NC, 1, true>(tw, l, tid, ld_w, st_g);
+      __syncthreads();  // W is reused by the next inverse
+    };
+    auto refill = [&]() {  // F is consumed: refill this input stage with the tile two ahead
+      if (threadIdx.x == 0) {
+        const int t2 = t + 2 * gridDim.x;
+        if (t2 < ntiles) issue(t2, s);
+      }
+    };
+    mbar_wait(&bar[s], (it >> 1) & 1, a.err);
+    if constexpr (ONE) {
+      float2 u[M];
+      // forward first stage in place; last stage, operator and inverse first
+      // stage in registers; inverse last stage to the output
+      ct_stage<NC, 0, false>(F, tw, l, tid, lay);
+      ct_fwd_last_to_regs<NC>(F, tw, l, tid, lay, u);
+      apply(setup(0), u);
+      ct_inv_first_from_regs<NC>(u, W, l, tid, lay);
+      fence_async_smem();
       __syncthreads();
-    }
-    // F is consumed: refill this input stage with the tile two ahead
-    fence_async_smem();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int t2 = t + 2 * gridDim.x;
-      if (t2 < ntiles) issue(t2, s);
+      refill();
+      finish(0);
+    } else {
+      // several outputs of one input: the forward transform stays in F, each
+      // output is multiplied into W and transformed back from there
+      ct_fft<NC, false, true, TL>(F, tw, lay);
+#pragma unroll 1
+      for (int q = 0; q < a.fanout; ++q) {
+        const OpEval ev = setup(q);
+#pragma unroll 4
+        for (int p = tid; p < NC; p += TPL) {
+          const float k2 = kxy2 + kl2[p];
+          float f;
+          if constexpr (CLS == FC_GRAD) {
+            f = ev.kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
+          } else if constexpr (CLS == FC_NABLA) {
+            f = (k2 == 0.f) ? (ev.e == 0.f ? T.scale : 0.f) : exp2f(ev.e * log2f(k2)) * T.scale;
+          } else {
+            f = cos_sq(cdt2sq * k2) * T.scale;
+          }
+          float2 v = c_scale(F[lay(l, p)], f);
+          if constexpr (CLS == FC_GRAD) v = c_mul(v, ev.dline ? ev.dline[p] : ev.dconst);
+          W[lay(l, p)] = v;
+        }
+        if (q + 1 == a.fanout) fence_async_smem();
+        __syncthreads();
+        if (q + 1 == a.fanout) refill();
+        ct_stage<NC, 0, true>(W, tw, l, tid, lay);
+        finish(q);
+      }
     }
   }
 }
@@ -297,11 +346,11 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
   return cudaGetLastError();
 }
 
-template <int NC, int CLS>
+template <int NC, int CLS, bool ONE>
 static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
                     NC * sizeof(float);
-  auto k = k_fused_tma<NC, CLS>;
+  auto k = k_fused_tma<NC, CLS, ONE>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
@@ -314,10 +363,12 @@ static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const Sp
 template <int NC>
 static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   const int kind = a.op[0].kind;
+  const bool one = a.fanout == 1;
   if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA || kind == OP_SHIFT_NEG)
-    return fused_tma_t<NC, FC_GRAD>(a, tw, T, st);
-  if (kind == OP_NABLA1 || kind == OP_NABLA2) return fused_tma_t<NC, FC_NABLA>(a, tw, T, st);
-  return fused_tma_t<NC, FC_SRCK>(a, tw, T, st);
+    return one ? fused_tma_t<NC, FC_GRAD, true>(a, tw, T, st) : fused_tma_t<NC, FC_GRAD, false>(a, tw, T, st);
+  if (kind == OP_NABLA1 || kind == OP_NABLA2)
+    return one ? fused_tma_t<NC, FC_NABLA, true>(a, tw, T, st) : fused_tma_t<NC, FC_NABLA, false>(a, tw, T, st);
+  return one ? fused_tma_t<NC, FC_SRCK, true>(a, tw, T, st) : fused_tma_t<NC, FC_SRCK, false>(a, tw, T, st);
 }
 
 int tma_lines(int n) { return ct_lines_of(n); }
