@@ -260,31 +260,20 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
       refill();
       finish(0);
     } else {
-      // several outputs of one input: the forward transform stays in F, each
-      // output is multiplied into W and transformed back from there
+      // several outputs of one input: the forward transform stays in F; each
+      // output is read from it in the hand-off order, multiplied in registers
+      // and given the inverse first stage on the way to W
       ct_fft<NC, false, true, TL>(F, tw, lay);
 #pragma unroll 1
       for (int q = 0; q < a.fanout; ++q) {
-        const OpEval ev = setup(q);
-#pragma unroll 4
-        for (int p = tid; p < NC; p += TPL) {
-          const float k2 = kxy2 + kl2[p];
-          float f;
-          if constexpr (CLS == FC_GRAD) {
-            f = ev.kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
-          } else if constexpr (CLS == FC_NABLA) {
-            f = (k2 == 0.f) ? (ev.e == 0.f ? T.scale : 0.f) : exp2f(ev.e * log2f(k2)) * T.scale;
-          } else {
-            f = cos_sq(cdt2sq * k2) * T.scale;
-          }
-          float2 v = c_scale(F[lay(l, p)], f);
-          if constexpr (CLS == FC_GRAD) v = c_mul(v, ev.dline ? ev.dline[p] : ev.dconst);
-          W[lay(l, p)] = v;
-        }
+        float2 u[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) u[m] = F[lay(l, tid + TPL * m)];
+        apply(setup(q), u);
+        ct_inv_first_from_regs<NC>(u, W, l, tid, lay);
         if (q + 1 == a.fanout) fence_async_smem();
         __syncthreads();
         if (q + 1 == a.fanout) refill();
-        ct_stage<NC, 0, true>(W, tw, l, tid, lay);
         finish(q);
       }
     }
