@@ -18,8 +18,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -68,15 +70,32 @@ static void ck(cudaError_t e, const char* what) {
 // ---------------------------------------------------------------------------
 // device buffer
 // ---------------------------------------------------------------------------
-DevBuf::~DevBuf() {
-  if (p) cudaFree(p);
+// Stream-ordered allocations from the device's default memory pool, which
+// keeps freed memory for the next session (set up once per device), so
+// creating and destroying sessions neither synchronises the device nor goes
+// back to the driver.  Buffers are freed on the legacy stream after the
+// session's own stream has been synchronised.
+static void retain_pool_memory() {
+  static std::once_flag once[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::call_once(once[dev], [dev] {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  });
 }
-void DevBuf::alloc(size_t nbytes) {
-  if (p) cudaFree(p);
+
+DevBuf::~DevBuf() {
+  if (p) cudaFreeAsync(p, nullptr);
+}
+void DevBuf::alloc(size_t nbytes, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
   p = nullptr;
   bytes = nbytes;
   if (nbytes == 0) return;
-  ck(cudaMalloc(&p, nbytes), "cudaMalloc");
+  ck(cudaMallocAsync(&p, nbytes, st), "cudaMallocAsync");
 }
 
 // ---------------------------------------------------------------------------
@@ -134,9 +153,28 @@ static std::vector<float> field_values(const kw_field& f) {
   return std::vector<float>(f.data, f.data + f.numel);
 }
 
+// Host loops over whole grids (medium maps built in FP64) split over the
+// host's threads: f(begin, end) on disjoint ranges.
+template <class F>
+static void parallel_for(size_t n, F&& f) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 64));
+  if (n < (1u << 16) || nt == 1) {
+    f(size_t(0), n);
+    return;
+  }
+  const size_t chunk = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (size_t t = 0; t < nt; ++t) {
+    const size_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) th.emplace_back([&f, a, b] { f(a, b); });
+  }
+  for (auto& x : th) x.join();
+}
+
 template <class T>
 static T* up(DevBuf& b, const T* h, size_t n, cudaStream_t st) {
-  b.alloc(n * sizeof(T));
+  b.alloc(n * sizeof(T), st);
   if (n) ck(cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
   return (T*)b.p;
 }
@@ -224,6 +262,7 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   if (in->p0_source_flag && in->p_source_flag)
     throw KwError(KW_ERR_INVALID_ARGUMENT, "p0 and p sources cannot be used together");
 
+  retain_pool_memory();
   ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
   ck(cudaEventCreate(&ev0), "cudaEventCreate");
   ck(cudaEventCreate(&ev1), "cudaEventCreate");
@@ -296,16 +335,21 @@ void Session::setup(const kw_input* in, const kw_options* o) {
 
   // ----- medium -----
   {
-    std::vector<float> c0 = field_values(in->c0);
-    std::vector<float> c0sq(c0.size());
-    for (size_t i = 0; i < c0.size(); ++i) c0sq[i] = c0[i] * c0[i];
+    const float* c0 = in->c0.data;
+    std::vector<float> c0sq(in->c0.numel);
+    parallel_for(c0sq.size(), [&](size_t a, size_t b) {
+      for (size_t i = a; i < b; ++i) c0sq[i] = c0[i] * c0[i];
+    });
     kw_field f{c0sq.data(), (uint64_t)c0sq.size()};
     c0sq_m = map_of(f, c0sq_buf, 0.f);
     rho0_m = map_of(in->rho0, rho0_buf, 0.f);
     const kw_field* sg[3] = {&in->rho0_sgx, &in->rho0_sgy, &in->rho0_sgz};
     for (int a = 0; a < d.dim; ++a) {
-      std::vector<float> v = field_values(*sg[a]);
-      for (auto& x : v) x = 1.0f / x;
+      std::vector<float> v(sg[a]->numel);
+      const float* src = sg[a]->data;
+      parallel_for(v.size(), [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i) v[i] = 1.0f / src[i];
+      });
       kw_field g{v.data(), (uint64_t)v.size()};
       rinv_m[a] = map_of(g, rinv_buf[a], 0.f);
     }
@@ -314,22 +358,28 @@ void Session::setup(const kw_input* in, const kw_options* o) {
       const bool het = in->c0.numel > 1 || in->alpha_coeff.numel > 1;
       const size_t n = het ? (size_t)d.npts : 1;
       const double y = in->alpha_power;
+      // db2neper is linear in the coefficient; tan(pi y / 2) is a constant
+      const double np_per_db = db2neper(1.0, eos == 1 ? y : 2.0);
+      const double tan_py = std::tan(M_PI * y / 2.0);
       std::vector<float> ctau(n), ceta(n);
-      for (size_t i = 0; i < n; ++i) {
-        const double c = in->c0.numel > 1 ? (double)in->c0.data[i] : (double)in->c0.data[0];
-        const double al = in->alpha_coeff.numel > 1 ? (double)in->alpha_coeff.data[i] : (double)in->alpha_coeff.data[0];
-        const double csq = (double)((float)c * (float)c);
-        if (eos == 1) {
-          const double a = db2neper(al, y);
-          const double tau = -2.0 * a * std::pow(c, y - 1.0);
-          const double eta = 2.0 * a * std::pow(c, y) * std::tan(M_PI * y / 2.0);
-          ctau[i] = (float)(csq * (double)(float)tau);
-          ceta[i] = (float)(csq * (double)(float)eta);
-        } else {
-          const double a = db2neper(al, 2.0);
-          ctau[i] = (float)(-2.0 * a * c);  // stokes: tau itself
+      parallel_for(n, [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i) {
+          const double c = in->c0.numel > 1 ? (double)in->c0.data[i] : (double)in->c0.data[0];
+          const double al =
+              in->alpha_coeff.numel > 1 ? (double)in->alpha_coeff.data[i] : (double)in->alpha_coeff.data[0];
+          const double a = al * np_per_db;
+          if (eos == 1) {
+            const double csq = (double)((float)c * (float)c);
+            const double cy1 = std::pow(c, y - 1.0);
+            const double tau = -2.0 * a * cy1;
+            const double eta = 2.0 * a * cy1 * c * tan_py;
+            ctau[i] = (float)(csq * (double)(float)tau);
+            ceta[i] = (float)(csq * (double)(float)eta);
+          } else {
+            ctau[i] = (float)(-2.0 * a * c);  // stokes: tau itself
+          }
         }
-      }
+      });
       kw_field ft{ctau.data(), (uint64_t)n}, fe{ceta.data(), (uint64_t)n};
       if (eos == 1) {
         c2tau_m = map_of(ft, c2tau_buf, 0.f);
@@ -344,16 +394,16 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   const size_t fb = sizeof(float) * d.npts;
   const size_t sb = sizeof(float2) * (size_t)d.nxp * d.nrows;
   for (int a = 0; a < d.dim; ++a) {
-    u_buf[a].alloc(fb);
-    rho_buf[a].alloc(fb);
+    u_buf[a].alloc(fb, st);
+    rho_buf[a].alloc(fb, st);
     ck(cudaMemsetAsync(u_buf[a].p, 0, fb, st), "memset");
     ck(cudaMemsetAsync(rho_buf[a].p, 0, fb, st), "memset");
   }
   for (int s = 0; s < 4; ++s) {
-    S_buf[s].alloc(sb);
+    S_buf[s].alloc(sb, st);
     ck(cudaMemsetAsync(S_buf[s].p, 0, sb, st), "memset");
   }
-  err_buf.alloc(sizeof(int));
+  err_buf.alloc(sizeof(int), st);
   ck(cudaMemsetAsync(err_buf.p, 0, sizeof(int), st), "memset");
   const char* no_graph = std::getenv("KWAVE_B200_NO_GRAPH");
   use_graph = !(no_graph && no_graph[0] == '1');
@@ -378,13 +428,13 @@ void Session::setup(const kw_input* in, const kw_options* o) {
     const int nslab = (d.nz + zs - 1) / zs;
     slab = (d.nz + nslab - 1) / nslab;
   }
-  if (eos == 1) ploc_buf.alloc(fb);
+  if (eos == 1) ploc_buf.alloc(fb, st);
   if (opt.p_final) {
-    p_buf.alloc(fb);
+    p_buf.alloc(fb, st);
     ck(cudaMemsetAsync(p_buf.p, 0, fb, st), "memset");
   }
   int one = 1;
-  clock_buf.alloc(sizeof(int));
+  clock_buf.alloc(sizeof(int), st);
   ck(cudaMemcpyAsync(clock_buf.p, &one, sizeof(int), cudaMemcpyHostToDevice, st), "clock");
   clk.t = (const int*)clock_buf.p;
   clk.start = (int)opt.start_index;
@@ -420,7 +470,7 @@ void Session::setup_sources(const kw_input* in) {
       pdense.len = p_len;
       if (nsig == 1) {
         // single signal: the corrected field is sig(t) * F^-1{cos(.) F{mask}}
-        psrc_field.alloc(sizeof(float) * d.npts);
+        psrc_field.alloc(sizeof(float) * d.npts, st);
         std::vector<float> ones(1, 1.0f);
         DevBuf onebuf;
         const float* d1 = up(onebuf, ones.data(), 1, st);
@@ -429,7 +479,7 @@ void Session::setup_sources(const kw_input* in) {
         pdense.field = (const float*)psrc_field.p;
         pdense.sig = dsig;
       } else {
-        psrc_field.alloc(sizeof(float) * d.npts);
+        psrc_field.alloc(sizeof(float) * d.npts, st);
         pdense.field = (const float*)psrc_field.p;
         pdense.sig = nullptr;
         p_many_additive = true;
@@ -474,7 +524,7 @@ void Session::setup_sources(const kw_input* in) {
       for (int a = 0; a < d.dim; ++a) {
         if (!uf[a]) continue;
         udense[a].len = u_len[a];
-        ufield_buf[a].alloc(sizeof(float) * d.npts);
+        ufield_buf[a].alloc(sizeof(float) * d.npts, st);
         udense[a].field = (const float*)ufield_buf[a].p;
         if (nsig == 1) {
           if (!ones_ready) {
@@ -674,7 +724,7 @@ void Session::setup_sensors(const kw_input* in) {
   const size_t per = sizeof(float) * (size_t)ns;
   const size_t all = sizeof(float) * (size_t)d.npts;
   auto zalloc = [&](DevBuf& b, size_t n) -> void* {
-    b.alloc(n);
+    b.alloc(n, st);
     if (n) ck(cudaMemsetAsync(b.p, 0, n, st), "memset");
     return b.p;
   };
@@ -711,7 +761,7 @@ void Session::setup_sensors(const kw_input* in) {
       mk(sens_uns[a]);
       sens_uns[a].raw = (float*)zalloc(uns_raw_buf[a], ser);
     }
-    uns_field_buf.alloc(all);
+    uns_field_buf.alloc(all, st);
   }
 }
 

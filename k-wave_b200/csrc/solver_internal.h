@@ -27,7 +27,7 @@ struct DevBuf {
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf();
-  void alloc(size_t nbytes);
+  void alloc(size_t nbytes, cudaStream_t st);
 };
 
 class Session {
