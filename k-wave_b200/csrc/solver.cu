@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -21,7 +22,6 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -54,6 +54,10 @@ cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& cl
                                 cudaStream_t st);
 cudaError_t launch_advance(int* t, cudaStream_t st);
 cudaError_t launch_rms_final(const float2* acc, float* out, long long n, float inv_n, cudaStream_t st);
+cudaError_t launch_medium_maps(float* c0_to_c0sq, float c0_scalar, float* ctau, float* ceta, const float* alpha,
+                               float alpha_scalar, double np_per_db, double y, double tan_py, int eos, long long n,
+                               cudaStream_t st);
+cudaError_t launch_reciprocal(float* v, long long n, cudaStream_t st);
 bool tma_supported(int n);
 int tma_lines(int n);
 bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n);
@@ -153,25 +157,6 @@ static std::vector<float> field_values(const kw_field& f) {
   return std::vector<float>(f.data, f.data + f.numel);
 }
 
-// Host loops over whole grids (medium maps built in FP64) split over the
-// host's threads: f(begin, end) on disjoint ranges.
-template <class F>
-static void parallel_for(size_t n, F&& f) {
-  const unsigned hw = std::thread::hardware_concurrency();
-  const size_t nt = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 64));
-  if (n < (1u << 16) || nt == 1) {
-    f(size_t(0), n);
-    return;
-  }
-  const size_t chunk = (n + nt - 1) / nt;
-  std::vector<std::thread> th;
-  for (size_t t = 0; t < nt; ++t) {
-    const size_t a = t * chunk, b = std::min(n, a + chunk);
-    if (a < b) th.emplace_back([&f, a, b] { f(a, b); });
-  }
-  for (auto& x : th) x.join();
-}
-
 template <class T>
 static T* up(DevBuf& b, const T* h, size_t n, cudaStream_t st) {
   b.alloc(n * sizeof(T), st);
@@ -219,9 +204,26 @@ static void sort_indices(const uint64_t* idx1, uint64_t n, uint64_t npts, std::v
   }
 }
 
+// Set-up phase timings on stderr at --verbose 2 (host wall time, the
+// device work of each phase included).
+struct PhaseTimer {
+  bool on;
+  cudaStream_t st = nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  void mark(const char* what) {
+    if (!on) return;
+    if (st) cudaStreamSynchronize(st);
+    const auto t = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "kwave_b200 set-up: %-28s %8.1f ms\n", what,
+                 std::chrono::duration<double, std::milli>(t - t0).count());
+    t0 = t;
+  }
+};
+
 void Session::setup(const kw_input* in, const kw_options* o) {
   if (!in || !o) throw KwError(KW_ERR_INVALID_ARGUMENT, "input and options must not be NULL");
   opt = *o;
+  PhaseTimer timer{opt.verbose >= 2};
   if (opt.start_index == 0) opt.start_index = 1;
   if (in->Nx < 1 || in->Ny < 1 || in->Nz < 1 || in->Nt < 1)
     throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
@@ -267,6 +269,8 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   ck(cudaEventCreate(&ev0), "cudaEventCreate");
   ck(cudaEventCreate(&ev1), "cudaEventCreate");
 
+  timer.st = st;
+  timer.mark("validation, stream");
   // ----- FFT plans and twiddles (FP64 -> FP32) -----
   const int ns[3] = {d.nx, d.ny, d.nz};
   for (int a = 0; a < d.dim; ++a) {
@@ -333,63 +337,71 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   T.ym1 = (float)(in->alpha_power - 1.0);
   dtf = in->dt;
 
+  timer.mark("plans, operator tables");
   // ----- medium -----
+  // Maps are uploaded as given and derived on the device (c0^2, 1/rho0_sg,
+  // and the FP64 absorption maps), scalars stay scalars.
   {
-    const float* c0 = in->c0.data;
-    std::vector<float> c0sq(in->c0.numel);
-    parallel_for(c0sq.size(), [&](size_t a, size_t b) {
-      for (size_t i = a; i < b; ++i) c0sq[i] = c0[i] * c0[i];
-    });
-    kw_field f{c0sq.data(), (uint64_t)c0sq.size()};
-    c0sq_m = map_of(f, c0sq_buf, 0.f);
+    const bool c0_map = in->c0.numel > 1;
+    if (c0_map) {
+      c0sq_m.p = up(c0sq_buf, in->c0.data, (size_t)in->c0.numel, st);  // squared below
+      c0sq_m.s = 0.f;
+    } else {
+      c0sq_m = Map{nullptr, in->c0.data[0] * in->c0.data[0]};
+    }
     rho0_m = map_of(in->rho0, rho0_buf, 0.f);
     const kw_field* sg[3] = {&in->rho0_sgx, &in->rho0_sgy, &in->rho0_sgz};
     for (int a = 0; a < d.dim; ++a) {
-      std::vector<float> v(sg[a]->numel);
-      const float* src = sg[a]->data;
-      parallel_for(v.size(), [&](size_t i0, size_t i1) {
-        for (size_t i = i0; i < i1; ++i) v[i] = 1.0f / src[i];
-      });
-      kw_field g{v.data(), (uint64_t)v.size()};
-      rinv_m[a] = map_of(g, rinv_buf[a], 0.f);
-    }
-    if (nonlinear) bona_m = map_of(in->BonA, bona_buf, 0.f);
-    if (eos == 1 || eos == 2) {
-      const bool het = in->c0.numel > 1 || in->alpha_coeff.numel > 1;
-      const size_t n = het ? (size_t)d.npts : 1;
-      const double y = in->alpha_power;
-      // db2neper is linear in the coefficient; tan(pi y / 2) is a constant
-      const double np_per_db = db2neper(1.0, eos == 1 ? y : 2.0);
-      const double tan_py = std::tan(M_PI * y / 2.0);
-      std::vector<float> ctau(n), ceta(n);
-      parallel_for(n, [&](size_t i0, size_t i1) {
-        for (size_t i = i0; i < i1; ++i) {
-          const double c = in->c0.numel > 1 ? (double)in->c0.data[i] : (double)in->c0.data[0];
-          const double al =
-              in->alpha_coeff.numel > 1 ? (double)in->alpha_coeff.data[i] : (double)in->alpha_coeff.data[0];
-          const double a = al * np_per_db;
-          if (eos == 1) {
-            const double csq = (double)((float)c * (float)c);
-            const double cy1 = std::pow(c, y - 1.0);
-            const double tau = -2.0 * a * cy1;
-            const double eta = 2.0 * a * cy1 * c * tan_py;
-            ctau[i] = (float)(csq * (double)(float)tau);
-            ceta[i] = (float)(csq * (double)(float)eta);
-          } else {
-            ctau[i] = (float)(-2.0 * a * c);  // stokes: tau itself
-          }
-        }
-      });
-      kw_field ft{ctau.data(), (uint64_t)n}, fe{ceta.data(), (uint64_t)n};
-      if (eos == 1) {
-        c2tau_m = map_of(ft, c2tau_buf, 0.f);
-        c2eta_m = map_of(fe, c2eta_buf, 0.f);
+      if (sg[a]->numel > 1) {
+        float* v = up(rinv_buf[a], sg[a]->data, (size_t)sg[a]->numel, st);
+        ck(launch_reciprocal(v, (long long)sg[a]->numel, st), "1/rho0_sg");
+        rinv_m[a] = Map{v, 0.f};
       } else {
-        tau_m = map_of(ft, c2tau_buf, 0.f);
+        rinv_m[a] = Map{nullptr, 1.0f / sg[a]->data[0]};
       }
     }
+    if (nonlinear) bona_m = map_of(in->BonA, bona_buf, 0.f);
+    float* ctau = nullptr;
+    float* ceta = nullptr;
+    const double y = in->alpha_power;
+    const double np_per_db = db2neper(1.0, eos == 1 ? y : 2.0);  // linear in the coefficient
+    const double tan_py = std::tan(M_PI * y / 2.0);
+    const bool absorb = eos == 1 || eos == 2;
+    const bool het = absorb && (c0_map || in->alpha_coeff.numel > 1);
+    DevBuf alpha_tmp;
+    const float* alpha_d = nullptr;
+    if (het) {
+      ctau = (float*)(c2tau_buf.alloc(sizeof(float) * d.npts, st), c2tau_buf.p);
+      if (eos == 1) ceta = (float*)(c2eta_buf.alloc(sizeof(float) * d.npts, st), c2eta_buf.p);
+      if (in->alpha_coeff.numel > 1) alpha_d = up(alpha_tmp, in->alpha_coeff.data, (size_t)in->alpha_coeff.numel, st);
+    }
+    if (c0_map || het)
+      ck(launch_medium_maps(c0_map ? (float*)c0sq_buf.p : nullptr, in->c0.data[0], ctau, ceta, alpha_d,
+                            in->alpha_coeff.numel ? in->alpha_coeff.data[0] : 0.f, np_per_db, y, tan_py, eos,
+                            d.npts, st),
+         "medium maps");
+    if (absorb && !het) {  // scalar medium: the same formulas on the host
+      const double c = in->c0.data[0];
+      const double al = in->alpha_coeff.data[0] * np_per_db;
+      const double csq = (double)((float)c * (float)c);
+      if (eos == 1) {
+        const double cy1 = std::pow(c, y - 1.0);
+        c2tau_m = Map{nullptr, (float)(csq * (double)(float)(-2.0 * al * cy1))};
+        c2eta_m = Map{nullptr, (float)(csq * (double)(float)(2.0 * al * cy1 * c * tan_py))};
+      } else {
+        tau_m = Map{nullptr, (float)(-2.0 * al * c)};
+      }
+    } else if (het) {
+      if (eos == 1) {
+        c2tau_m = Map{ctau, 0.f};
+        c2eta_m = Map{ceta, 0.f};
+      } else {
+        tau_m = Map{ctau, 0.f};
+      }
+    }
+    if (alpha_tmp.p) ck(cudaStreamSynchronize(st), "medium maps");  // alpha_tmp is freed on leaving
   }
-
+  timer.mark("medium maps");
   // ----- fields and spectral work buffers -----
   const size_t fb = sizeof(float) * d.npts;
   const size_t sb = sizeof(float2) * (size_t)d.nxp * d.nrows;
@@ -439,13 +451,16 @@ void Session::setup(const kw_input* in, const kw_options* o) {
   clk.t = (const int*)clock_buf.p;
   clk.start = (int)opt.start_index;
 
+  timer.mark("fields, TMA maps, clock");
   // ----- sources -----
   p0 = in->p0_source_flag != 0;
   if (p0) up(p0_buf, in->p0_source_input, (size_t)d.npts, st);
   setup_sources(in);
 
+  timer.mark("sources");
   // ----- sensors -----
   setup_sensors(in);
+  timer.mark("sensors");
   ck(cudaStreamSynchronize(st), "setup");
 }
 
@@ -685,8 +700,7 @@ void Session::setup_sensors(const kw_input* in) {
     if (!in->sensor_mask_index || in->sensor_mask_index_numel == 0)
       throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_index missing");
     ns = (long long)in->sensor_mask_index_numel;
-    std::vector<uint64_t> lin(in->sensor_mask_index, in->sensor_mask_index + ns);
-    build_sensor_lists(lin, si, sl);
+    build_sensor_lists(in->sensor_mask_index, (size_t)ns, si, sl);
   } else if (in->sensor_mask_type == 1) {
     if (!in->sensor_mask_corners || in->sensor_mask_corners_numel == 0 || in->sensor_mask_corners_numel % 6)
       throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_corners must hold 6 values per cuboid");
@@ -705,7 +719,7 @@ void Session::setup_sensors(const kw_input* in) {
             lin.push_back((x - 1) + (uint64_t)d.nx * ((y - 1) + (uint64_t)d.ny * (z - 1)) + 1);
     }
     ns = (long long)lin.size();
-    build_sensor_lists(lin, si, sl);
+    build_sensor_lists(lin.data(), lin.size(), si, sl);
   } else {
     throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_type must be 0 or 1");
   }
@@ -782,9 +796,9 @@ void Session::record_non_staggered() {
   }
 }
 
-void Session::build_sensor_lists(const std::vector<uint64_t>& lin, std::vector<int>& si, std::vector<int>& sl) {
+void Session::build_sensor_lists(const uint64_t* lin, size_t n, std::vector<int>& si, std::vector<int>& sl) {
   // dense identity: every grid point in linear order
-  dense_sensor = ((long long)lin.size() == d.npts);
+  dense_sensor = ((long long)n == d.npts);
   if (dense_sensor)
     for (long long j = 0; j < d.npts; ++j)
       if (lin[j] != (uint64_t)j + 1) {
@@ -792,8 +806,8 @@ void Session::build_sensor_lists(const std::vector<uint64_t>& lin, std::vector<i
         break;
       }
   if (dense_sensor) return;
-  std::vector<std::pair<long long, int>> v(lin.size());
-  for (size_t j = 0; j < lin.size(); ++j) {
+  std::vector<std::pair<long long, int>> v(n);
+  for (size_t j = 0; j < n; ++j) {
     if (lin[j] < 1 || lin[j] > (uint64_t)d.npts)
       throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_index holds an index outside the grid");
     v[j] = {(long long)lin[j] - 1, (int)j};

@@ -56,7 +56,7 @@ class Session {
   Map map_of(const kw_field& f, DevBuf& buf, float scalar_default);
   void setup_sources(const kw_input* in);
   void setup_sensors(const kw_input* in);
-  void build_sensor_lists(const std::vector<uint64_t>& lin, std::vector<int>& si, std::vector<int>& sl);
+  void build_sensor_lists(const uint64_t* lin, size_t n, std::vector<int>& si, std::vector<int>& sl);
   void corrected_source(float* out, const int* idx, const int* slot, int n, const float* sig, int nrows_sig,
                         int t);
   void corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
