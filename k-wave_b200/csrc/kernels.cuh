@@ -89,6 +89,7 @@ struct DenseSource {
 struct Sensor {
   int mode;
   int ns;
+  int ring;        // raw series rows held on the device (0: every recorded step)
   const int* idx;
   const int* slot;
   float* raw;      // [nrec][ns] time series (nullptr: off)

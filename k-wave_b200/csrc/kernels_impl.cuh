@@ -291,8 +291,14 @@ __device__ __forceinline__ void tile_range(const int* idx, int n, long long a, l
   __syncthreads();
 }
 
+// Row of the raw series that record index fi (1-based) goes to: a ring of
+// s.ring rows when the series is streamed to the host in blocks.
+__device__ __forceinline__ long long raw_row(const Sensor& s, int fi) {
+  return s.ring ? (long long)((fi - 1) % s.ring) : (long long)(fi - 1);
+}
+
 __device__ __forceinline__ void sensor_put(const Sensor& s, int fi, long long slot, float v) {
-  if (s.raw) s.raw[(long long)(fi - 1) * s.ns + slot] = v;
+  if (s.raw) s.raw[raw_row(s, fi) * s.ns + slot] = v;
   if (s.vmax) s.vmax[slot] = (fi == 1) ? v : fmaxf(s.vmax[slot], v);
   if (s.vmin) s.vmin[slot] = (fi == 1) ? v : fminf(s.vmin[slot], v);
   if (s.rms) {
@@ -347,7 +353,7 @@ __device__ __forceinline__ float2 kahan_add(float2 acc, float v) {
 __device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long gi, float4 v) {
   if (fi <= 0) return;
   if (s.mode == 1) {
-    if (s.raw) st4(s.raw, (long long)(fi - 1) * s.ns + gi, v);
+    if (s.raw) st4(s.raw, raw_row(s, fi) * s.ns + gi, v);
     if (s.vmax) st4(s.vmax, gi, fi == 1 ? v : max4(ld4(s.vmax, gi), v));
     if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
     if (s.rms) {

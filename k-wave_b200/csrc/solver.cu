@@ -220,7 +220,8 @@ struct PhaseTimer {
   }
 };
 
-void Session::setup(const kw_input* in, const kw_options* o) {
+void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
+  allow_ring_ = allow_ring;
   if (!in || !o) throw KwError(KW_ERR_INVALID_ARGUMENT, "input and options must not be NULL");
   opt = *o;
   PhaseTimer timer{opt.verbose >= 2};
@@ -725,16 +726,38 @@ void Session::setup_sensors(const kw_input* in) {
   }
   if (opt.start_index > Nt) nrec = 0;
   else nrec = (long long)(Nt - opt.start_index + 1);
+  // Raw series (p, u, u on the regular grid) recorded every step can exceed
+  // the device: when streaming is allowed and they would take more than the
+  // recording budget (KWAVE_B200_RECORD_BUDGET bytes, default a quarter of the
+  // device memory), only a ring of steps is kept on the device and the caller
+  // drains it in blocks.
+  {
+    const long long streams = (opt.p_raw ? 1 : 0) + d.dim * ((opt.u_raw ? 1 : 0) + (opt.u_non_staggered_raw ? 1 : 0));
+    const double per_step = 4.0 * (double)ns * (double)streams;
+    double budget = 0.0;
+    if (const char* e = std::getenv("KWAVE_B200_RECORD_BUDGET")) budget = std::atof(e);
+    if (!(budget > 0)) {
+      size_t fr = 0, tot = 0;
+      budget = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? 0.25 * (double)tot : 16e9;
+    }
+    ring_rows = 0;
+    if (allow_ring_ && streams && nrec > 0 && per_step * (double)nrec > budget)
+      ring_rows = std::max<long long>(1, std::min<long long>(nrec, (long long)(budget / per_step)));
+    drained = 0;
+  }
   // sensor state for p and u
   auto mk = [&](Sensor& s) {
     s = Sensor{};
     s.mode = dense_sensor ? 1 : 2;
     s.ns = (int)ns;
+    s.ring = (int)ring_rows;
     s.idx = dense_sensor ? nullptr : sidx_d;
     s.slot = dense_sensor ? nullptr : sslot_d;
   };
   mk(sens_p);
-  const size_t ser = sizeof(float) * (size_t)ns * (size_t)nrec;
+  const size_t ser = sizeof(float) * (size_t)ns * (size_t)(ring_rows ? ring_rows : nrec);
+  if (ring_rows && sens_p.ring != ring_rows)
+    throw KwError(KW_ERR_INTERNAL, "streamed series: sensor ring not set");
   const size_t per = sizeof(float) * (size_t)ns;
   const size_t all = sizeof(float) * (size_t)d.npts;
   auto zalloc = [&](DevBuf& b, size_t n) -> void* {
@@ -1029,6 +1052,10 @@ void Session::corrected_source_into(float* out, const int* idx, const int* slot,
 
 void Session::advance(uint64_t n) {
   if (t_done + n > Nt) throw KwError(KW_ERR_INVALID_ARGUMENT, "advance beyond Nt");
+  if (ring_rows) {  // rows recorded but not yet drained must still fit the ring
+    const long long after = std::min<long long>(nrec, std::max<long long>(0, (long long)(t_done + n) - (long long)opt.start_index + 1));
+    if (after - drained > ring_rows) throw KwError(KW_ERR_INVALID_ARGUMENT, "drain the streamed series before advancing further");
+  }
   ck(cudaEventRecord(ev0, st), "event");
   const uint64_t l0 = launches_;
   for (uint64_t i = 0; i < n; ++i) enqueue_step();
@@ -1178,14 +1205,36 @@ static void d2h(float* dst, const void* src, size_t n, cudaStream_t st) {
   if (dst && src && n) ck(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost, st), "d2h");
 }
 
+void Session::drain_raw(kw_output* out) {
+  if (!ring_rows) return;
+  const long long nr = std::min<long long>(nrec, std::max<long long>(0, (long long)t_done - (long long)opt.start_index + 1));
+  float* dst[10] = {out->p, out->ux, out->uy, out->uz, out->ux_non_staggered, out->uy_non_staggered,
+                    out->uz_non_staggered, nullptr, nullptr, nullptr};
+  const void* src[10] = {p_raw_buf.p, u_raw_buf[0].p, u_raw_buf[1].p, u_raw_buf[2].p, uns_raw_buf[0].p,
+                         uns_raw_buf[1].p, uns_raw_buf[2].p, nullptr, nullptr, nullptr};
+  for (long long r = drained; r < nr;) {
+    const long long slot = r % ring_rows;
+    const long long cnt = std::min(nr - r, ring_rows - slot);  // contiguous up to the ring's end
+    for (int k = 0; k < 7; ++k)
+      if (dst[k] && src[k])
+        ck(cudaMemcpyAsync(dst[k] + (size_t)r * ns, (const float*)src[k] + (size_t)slot * ns,
+                           sizeof(float) * (size_t)cnt * (size_t)ns, cudaMemcpyDeviceToHost, st),
+           "drain");
+    r += cnt;
+  }
+  ck(cudaStreamSynchronize(st), "drain");
+  drained = nr;
+}
+
 void Session::read(kw_output* out) {
   if (!out) throw KwError(KW_ERR_INVALID_ARGUMENT, "output must not be NULL");
+  drain_raw(out);
   const long long nr = std::min<long long>(nrec, std::max<long long>(0, (long long)t_done - (long long)opt.start_index + 1));
   const float inv = nr > 0 ? 1.0f / (float)nr : 0.f;
   if (p_rms_buf.p) ck(launch_rms_final((const float2*)p_rms_buf.p, (float*)p_rmsf_buf.p, ns, inv, st), "rms");
   for (int a = 0; a < d.dim; ++a)
     if (u_rms_buf[a].p) ck(launch_rms_final((const float2*)u_rms_buf[a].p, (float*)u_rmsf_buf[a].p, ns, inv, st), "rms");
-  const size_t ser = (size_t)ns * (size_t)nrec, per = (size_t)ns, all = (size_t)d.npts;
+  const size_t ser = ring_rows ? 0 : (size_t)ns * (size_t)nrec, per = (size_t)ns, all = (size_t)d.npts;
   d2h(out->p, p_raw_buf.p, ser, st);
   d2h(out->p_max, p_max_buf.p, per, st);
   d2h(out->p_min, p_min_buf.p, per, st);
@@ -1398,8 +1447,15 @@ int kw_solve(const kw_input* in, const kw_options* opt, kw_output* out, kw_statu
   return guarded(status, [&] {
     select_device(opt);
     Session s;
-    s.setup(in, opt);
-    s.advance(s.Nt);
+    s.setup(in, opt, /*allow_ring=*/true);
+    if (!s.ring_rows) {
+      s.advance(s.Nt);
+    } else {  // streamed raw series: advance a ring's worth of steps, drain, repeat
+      while (s.t_done < s.Nt) {
+        s.advance(std::min<uint64_t>(s.Nt - s.t_done, (uint64_t)s.ring_rows));
+        s.drain_raw(out);
+      }
+    }
     s.read(out);
   });
 }

@@ -33,7 +33,13 @@ struct DevBuf {
 class Session {
  public:
   ~Session();
-  void setup(const kw_input* in, const kw_options* opt);
+  // allow_ring: the caller drains raw series in blocks (drain_raw), so they
+  // may be held on the device as a ring of steps when the full series would
+  // not fit the recording budget
+  void setup(const kw_input* in, const kw_options* opt, bool allow_ring = false);
+  void drain_raw(kw_output* out);  // copy raw rows recorded since the last drain
+  long long ring_rows = 0, drained = 0;
+  bool allow_ring_ = false;
   void advance(uint64_t n);
   float elapsed_ms();
   void sync();
