@@ -22,7 +22,7 @@ import numpy as np
 import scipy.fft as sfft
 
 from . import _lib
-from .utils import KWaveGrid, cart2grid, reorder_binary_sensor_data, smooth
+from .utils import KWaveGrid, cart2grid, cart_linear_weights, reorder_binary_sensor_data, smooth
 
 MODE = {"dirichlet": 0, "additive-no-correction": 1, "additive": 2}
 PML_DEFAULT = {2: (20, 2.0), 3: (10, 2.0)}  # kspaceFirstOrder_setDefaults.m:150-167
@@ -61,11 +61,19 @@ def _find(mask):
 
 
 def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_size=None,
-            pml_alpha=None, pml_inside=True, smooth_p0=True, data_cast="single"):
+            pml_alpha=None, pml_inside=True, smooth_p0=True, data_cast="single", cart_interp="nearest"):
     """Build the datasets of the HDF5 input file (saveToDisk.m:44-378)
     plus the record list / start index the wrapper turns into flags.
 
+    ``cart_interp`` is the reference's 'CartInterp' for Cartesian sensor
+    points: "nearest" maps them to grid points, the only form an input file
+    can hold (kspaceFirstOrder_saveToDisk.m:35-37); "linear" records the
+    vertices around each point and interpolates the series in postprocess()
+    (the in-memory solvers' default, kspaceFirstOrder_extractSensorData.m:296-420).
+
     Returns (inp, record, start_index, meta)."""
+    if cart_interp not in ("nearest", "linear"):
+        raise ValueError("cart_interp must be 'nearest' or 'linear'")
     if not pml_inside:
         raise NotImplementedError("PMLInside = false is not supported")
     dim = kgrid.dim
@@ -192,6 +200,14 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         inp["sensor_mask_corners"] = corners
         meta["cuboid"] = True
         meta["corners"] = corners
+    elif mask.ndim == 2 and mask.shape[0] == dim and cart_interp == "linear":
+        # Cartesian points, linear interpolation: record the vertices of the
+        # simplices holding the points, interpolate on the host
+        verts, w = cart_linear_weights(kgrid, mask)
+        uniq = np.unique(verts)
+        inp["sensor_mask_type"] = 0
+        inp["sensor_mask_index"] = uniq
+        meta["interp"] = {"col": np.searchsorted(uniq, verts), "w": w}
     elif mask.ndim == 2 and mask.shape[0] == dim:
         # Cartesian points: nearest-neighbour mapping, as the file path requires
         # (kspaceFirstOrder_saveToDisk.m:35-37; createStorageVariables.m:33-51)
@@ -205,6 +221,19 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         record = [r for r in record if r not in ("I", "I_avg")] + [r for r in ("u_non_staggered", "p")
                                                                    if r not in record]
         meta["intensity"] = [r for r in sensor["record"] if r in ("I", "I_avg")]
+    if meta.get("interp") is not None:
+        # the simplex vertices record whole series; per-point reductions are
+        # taken on the interpolated series (kspaceFirstOrder_extractSensorData.m)
+        grid_out = [r for r in record if r.endswith("_all") or r.endswith("_final")]
+        raw = []
+        if any(r in record for r in ("p", "p_max", "p_min", "p_rms")):
+            raw.append("p")
+        if any(r in record for r in ("u", "u_max", "u_min", "u_rms")):
+            raw.append("u")
+        if "u_non_staggered" in record:
+            raw.append("u_non_staggered")
+        meta["interp"]["record"] = list(record)
+        record = grid_out + raw
     start = int(sensor.get("record_start_index", 1))
     meta["user_record"] = list(sensor.get("record", ["p"]))
     meta["has_record"] = "record" in sensor
@@ -226,11 +255,39 @@ def fourier_shift(data, shift, axis=-1):
     return np.real(sfft.ifft(op * sfft.fft(data, axis=axis), axis=axis))
 
 
+def _interpolate_sensors(out, meta, dim):
+    """Cartesian sensors with linear interpolation: weighted sums of the
+    vertex series, then the requested per-point reductions of the
+    interpolated series."""
+    col, w, rec = meta["interp"]["col"], meta["interp"]["w"], meta["interp"]["record"]
+    series = ["p"] + [f"u{c}" for c in "xyz"[:dim]] + [f"u{c}_non_staggered" for c in "xyz"[:dim]]
+    for k in series:
+        if k in out:
+            v = np.asarray(out[k], dtype=np.float64)
+            out[k] = np.einsum("pj,pjt->pt", w, v[col]).astype(np.float32)
+    comps = {"p": ["p"], "u": [f"u{c}" for c in "xyz"[:dim]]}
+    for base, keys in comps.items():
+        for k in keys:
+            if k not in out:
+                continue
+            v = out[k].astype(np.float64)
+            if f"{base}_max" in rec:
+                out[f"{k}_max"] = v.max(axis=1).astype(np.float32)
+            if f"{base}_min" in rec:
+                out[f"{k}_min"] = v.min(axis=1).astype(np.float32)
+            if f"{base}_rms" in rec:
+                out[f"{k}_rms"] = np.sqrt(np.mean(v * v, axis=1)).astype(np.float32)
+            if base not in rec and not (base == "p" and meta.get("intensity")):
+                out.pop(k)
+
+
 def postprocess(out: dict, inp: dict, meta: dict):
     """Intensity, Cartesian reorder and cuboid reshape
     (kspaceFirstOrder_saveIntensity.m:42-75, _reorderCartData.m,
     _reorderCuboidCorners.m:33-272)."""
     dim = meta["dim"]
+    if meta.get("interp") is not None:
+        _interpolate_sensors(out, meta, dim)
     if meta.get("intensity"):
         for c in "xyz"[:dim]:
             u_sgt = fourier_shift(out[f"u{c}_non_staggered"], 0.5, axis=-1)

@@ -170,6 +170,44 @@ def cart2grid(kgrid: KWaveGrid, cart):
     return mask, order_index, reorder_index
 
 
+def cart_linear_weights(kgrid: KWaveGrid, cart):
+    """Linear interpolation of Cartesian points on a triangulation of the grid:
+    the cell around each point is split into triangles (2D: along the
+    diagonal from its lowest to its highest corner) or the six Kuhn
+    tetrahedra (3D), and the point gets the barycentric weights of the
+    simplex that holds it -- exact for fields linear in x, y, z.  The
+    reference triangulates the grid with MATLAB's Delaunay, which is
+    degenerate on a regular grid (four co-circular points per cell), so its
+    choice of diagonal can differ (kspaceFirstOrder_createStorageVariables.m:372-394,
+    gridDataFast2D.m).  Returns (vertices, weights): 1-based column-major
+    linear indices and weights, both (points, dim + 1)."""
+    cart = np.asarray(cart, dtype=np.float64)
+    dim = kgrid.dim
+    n = cart.shape[1]
+    f = np.empty((dim, n))
+    for a in range(dim):
+        f[a] = cart[a] / kgrid.d[a] + kgrid.N[a] // 2  # 0-based fractional index (x_vec of makeDim)
+        if f[a].min() < -1e-9 or f[a].max() > kgrid.N[a] - 1 + 1e-9:
+            raise ValueError("Cartesian points must lie within the grid defined by kgrid.")
+    f = np.clip(f, 0, np.array(kgrid.N, dtype=np.float64)[:, None] - 1)
+    i0 = np.minimum(np.floor(f).astype(np.int64), np.array(kgrid.N)[:, None] - 2)
+    t = f - i0  # in [0, 1]
+    order = np.argsort(-t, axis=0, kind="stable")  # axes by decreasing fraction
+    verts = np.zeros((n, dim + 1), dtype=np.int64)
+    w = np.zeros((n, dim + 1))
+    strides = np.cumprod([1] + list(kgrid.N[:-1]))
+    for j in range(n):
+        cur = i0[:, j].copy()
+        ts = t[order[:, j], j]
+        w[j, 0] = 1.0 - ts[0]
+        verts[j, 0] = int(np.dot(cur, strides)) + 1
+        for m in range(dim):
+            cur[order[m, j]] += 1
+            w[j, m + 1] = (ts[m] - ts[m + 1]) if m + 1 < dim else ts[m]
+            verts[j, m + 1] = int(np.dot(cur, strides)) + 1
+    return verts, w
+
+
 def reorder_binary_sensor_data(data, reorder_index):
     """reorderBinarySensorData.m: sortrows on the appended reorder index."""
     order = np.argsort(np.asarray(reorder_index), kind="stable")
