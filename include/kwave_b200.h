@@ -114,6 +114,20 @@ typedef struct {
   uint64_t sensor_mask_index_numel;
   const uint64_t* sensor_mask_corners; /* 6 x K, 1-based [x1 y1 z1 x2 y2 z2] per cuboid */
   uint64_t sensor_mask_corners_numel;  /* 6 * K */
+
+  /*
+   * Transducer source (3D; saveToDisk.m:289-293, 339-343): while the 1-based
+   * time index t <= transducer_source_flag, the x velocity at each point of
+   * u_source_index gains apodization[i] * transducer_source_input[delay_mask[i] + t - 2]
+   * (kspaceFirstOrder3D.m:886-902).  delay_mask is 1-based, one entry per
+   * u_source_index entry; the velocity source flags must then be 0.  The
+   * input file carries no apodization: NULL means 1 for every point.
+   */
+  uint64_t transducer_source_flag;
+  const float* transducer_source_input;
+  uint64_t transducer_source_input_numel;
+  const uint64_t* delay_mask;
+  const float* transducer_source_apodization;
 } kw_input;
 
 /* What to record, and run settings: the binary's command-line flags. */

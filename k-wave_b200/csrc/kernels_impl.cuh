@@ -553,6 +553,20 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
     }
     __syncthreads();
   }
+  // transducer source, after the velocity sources as in the reference loop
+  if (ax == 0 && a.tr.n > 0 && t <= a.tr.len && !a.init) {
+    const long long rend = min(r0 + 2LL * L, d.row1);
+    tile_range(a.tr.idx, a.tr.n, r0 * nx, rend * nx, sh);
+    const int lo = sh[0], hi = sh[1];
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+      const long long local = (long long)__ldg(a.tr.idx + j) - r0 * nx;
+      const int q = (int)(local / nx), x = (int)(local - (long long)q * nx);
+      const float w = a.tr.apod ? __ldg(a.tr.apod + j) : 1.f;
+      const float v = w * __ldg(a.tr.sig + __ldg(a.tr.delay + j) + (t - 1));
+      set_comp(G, lay, q, x, get_comp(G, lay, q, x) + v);
+    }
+    __syncthreads();
+  }
   const Sensor& s = a.sens[ax];
   if constexpr (VEC) {
 #pragma unroll 4

@@ -568,6 +568,41 @@ void Session::setup_sources(const kw_input* in) {
       usrc.len = 0;
     }
   }
+  // transducer source (kspaceFirstOrder_inputChecking.m:1155-1213 builds
+  // what the file holds; kspaceFirstOrder3D.m:886-902 applies it)
+  tsrc = TransducerSource{};
+  if (in->transducer_source_flag) {
+    if (d.dim != 3) throw KwError(KW_ERR_INVALID_ARGUMENT, "transducer sources are 3D only");
+    if (uf[0] || uf[1] || uf[2])
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "a transducer source excludes the velocity sources");
+    if (!in->u_source_index || in->u_source_index_numel == 0)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "u_source_index missing");
+    if (!in->delay_mask || !in->transducer_source_input)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "transducer source needs delay_mask and transducer_source_input");
+    if (in->transducer_source_flag > (uint64_t)INT32_MAX ||
+        in->transducer_source_input_numel > (uint64_t)INT32_MAX)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "transducer signal too long");
+    const uint64_t len = in->transducer_source_flag, nsig = in->transducer_source_input_numel;
+    std::vector<int> si, sl;
+    sort_indices(in->u_source_index, in->u_source_index_numel, d.npts, si, sl, "u_source_index");
+    std::vector<int> dl(si.size());
+    std::vector<float> ap;
+    if (in->transducer_source_apodization) ap.resize(si.size());
+    for (size_t j = 0; j < si.size(); ++j) {
+      const uint64_t dm = in->delay_mask[sl[j]];
+      // every sample read, delay_mask + t - 2 for t <= len, lies in the signal
+      if (dm < 1 || dm - 1 + len > nsig)
+        throw KwError(KW_ERR_INVALID_ARGUMENT, "delay_mask reads past the end of transducer_source_input");
+      dl[j] = (int)(dm - 1);
+      if (!ap.empty()) ap[j] = in->transducer_source_apodization[sl[j]];
+    }
+    tsrc.n = (int)si.size();
+    tsrc.idx = up(tsrc_idx, si.data(), si.size(), st);
+    tsrc.delay = up(tsrc_delay, dl.data(), dl.size(), st);
+    tsrc.apod = ap.empty() ? nullptr : up(tsrc_apod, ap.data(), ap.size(), st);
+    tsrc.sig = up(tsrc_sig, in->transducer_source_input, nsig, st);
+    tsrc.len = (int)len;
+  }
 }
 
 // out = real(ifftn(source_kappa .* fftn(scatter(sig(:, t)))))
@@ -895,6 +930,7 @@ UArgs Session::u_args(float2* const* S) {
   ua.init = 0;
   ua.do_r2c = 1;
   ua.src = usrc;
+  ua.tr = tsrc;
   ua.clk = clk;
   return ua;
 }

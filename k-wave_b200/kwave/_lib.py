@@ -57,6 +57,9 @@ class KwInput(C.Structure):
         ("sensor_mask_type", C.c_uint64),
         ("sensor_mask_index", c_u64_p), ("sensor_mask_index_numel", C.c_uint64),
         ("sensor_mask_corners", c_u64_p), ("sensor_mask_corners_numel", C.c_uint64),
+        ("transducer_source_flag", C.c_uint64), ("transducer_source_input", c_float_p),
+        ("transducer_source_input_numel", C.c_uint64), ("delay_mask", c_u64_p),
+        ("transducer_source_apodization", c_float_p),
     ]
 
 
@@ -246,12 +249,20 @@ def make_input(inp: dict):
             sig = np.asarray(inp[f"u{a}_source_input"], dtype=np.float32)
             sig = sig.reshape(-1, sig.shape[-1]) if sig.ndim > 1 else sig.reshape(1, -1)
             setattr(s, f"u{a}_source_input", _fptr(keep.f32(sig)))
-    if u_any:
-        s.u_source_mode = int(inp["u_source_mode"])
+    s.transducer_source_flag = int(inp.get("transducer_source_flag", 0))
+    if u_any or s.transducer_source_flag:
+        s.u_source_mode = int(inp.get("u_source_mode", 0))
         s.u_source_many = int(inp.get("u_source_many", 0))
         idx = keep.u64(inp["u_source_index"])
         s.u_source_index = _uptr(idx)
         s.u_source_index_numel = idx.size
+    if s.transducer_source_flag:
+        sig = keep.f32(inp["transducer_source_input"])
+        s.transducer_source_input = _fptr(sig)
+        s.transducer_source_input_numel = sig.size
+        s.delay_mask = _uptr(keep.u64(inp["delay_mask"]))
+        if inp.get("transducer_source_apodization") is not None:
+            s.transducer_source_apodization = _fptr(keep.f32(inp["transducer_source_apodization"]))
     s.sensor_mask_type = int(inp.get("sensor_mask_type", 0))
     if s.sensor_mask_type == 0:
         idx = keep.u64(inp["sensor_mask_index"])

@@ -19,6 +19,7 @@ from __future__ import annotations
 import datetime
 import mmap
 import struct
+import warnings
 import zlib
 
 import numpy as np
@@ -185,13 +186,15 @@ class Writer:
 
 FLOAT_VARS = ("dx", "dy", "dz", "pml_x_alpha", "pml_y_alpha", "pml_z_alpha", "dt", "c0", "c_ref", "rho0",
               "rho0_sgx", "rho0_sgy", "rho0_sgz", "BonA", "alpha_coeff", "alpha_power", "p_source_input",
-              "ux_source_input", "uy_source_input", "uz_source_input", "p0_source_input")
+              "ux_source_input", "uy_source_input", "uz_source_input", "p0_source_input",
+              "transducer_source_input")
 INT_VARS = ("Nx", "Ny", "Nz", "Nt", "p_source_flag", "p0_source_flag", "ux_source_flag", "uy_source_flag",
             "uz_source_flag", "sxx_source_flag", "syy_source_flag", "szz_source_flag", "sxy_source_flag",
             "sxz_source_flag", "syz_source_flag", "transducer_source_flag", "nonuniform_grid_flag",
             "nonlinear_flag", "absorbing_flag", "elastic_flag", "axisymmetric_flag", "sensor_mask_type",
             "pml_x_size", "pml_y_size", "pml_z_size", "p_source_mode", "p_source_many", "p_source_index",
-            "u_source_mode", "u_source_many", "u_source_index", "sensor_mask_index", "sensor_mask_corners")
+            "u_source_mode", "u_source_many", "u_source_index", "sensor_mask_index", "sensor_mask_corners",
+            "delay_mask")
 
 
 def _matlab_dims(v):
@@ -205,7 +208,14 @@ def _matlab_dims(v):
 
 def write_input_file(path, inp: dict, description="input written by kwave.h5io"):
     """Write the datasets of ``prepare()``'s input dict as a k-Wave v1.2
-    input file.  Arrays are given in MATLAB axis order (x first)."""
+    input file.  Arrays are given in MATLAB axis order (x first).
+
+    A transducer's transmit apodization has no dataset in the format (the
+    reference's writer, kspaceFirstOrder_saveToDisk.m:289-293, 339-343,
+    drops it too); it is left out with a warning unless it is all ones."""
+    apod = inp.get("transducer_source_apodization")
+    if apod is not None and np.any(np.asarray(apod) != 1):
+        warnings.warn("the input file format has no transmit apodization: it is dropped", stacklevel=2)
     w = Writer()
     dim3 = int(inp["Nz"]) > 1
     flags = {k: 0 for k in INT_VARS if k.endswith("_flag")}

@@ -22,6 +22,7 @@ import numpy as np
 import scipy.fft as sfft
 
 from . import _lib
+from .transducer import KWaveTransducer, transducer_source_datasets
 from .utils import KWaveGrid, cart2grid, cart_linear_weights, reorder_binary_sensor_data, smooth
 
 MODE = {"dirichlet": 0, "additive-no-correction": 1, "additive": 2}
@@ -60,6 +61,63 @@ def _find(mask):
     return np.flatnonzero(np.asarray(mask).reshape(-1, order="F")) + 1
 
 
+def _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0):
+    """PMLInside = false: the grid grows by the PML on every side
+    (kspaceFirstOrder_expandGridMatrices.m).  Medium maps extend their edge
+    values, masks and p0 grow with zeros (p0 smoothed first, as
+    kspaceFirstOrder_inputChecking.m:1499-1557 orders it), cuboid corners
+    shift; Cartesian points keep their coordinates, which the centred grid
+    preserves.  Returns the new grid, inputs and the slices that cut the
+    full-grid outputs back to the user's grid (kspaceFirstOrder3DC.m:586-614)."""
+    import copy
+
+    dim = kgrid.dim
+    pad = [(int(p), int(p)) for p in ps]
+    big = KWaveGrid(tuple(n + 2 * int(p) for n, p in zip(kgrid.N, ps)), kgrid.d)
+    big.set_time(kgrid.Nt, kgrid.dt)
+    trim = tuple(slice(int(p), int(p) + n) for p, n in zip(ps, kgrid.N))
+
+    def grid_shaped(a):
+        return np.ndim(a) == dim and tuple(np.shape(a)) == tuple(kgrid.N)
+
+    medium = dict(medium)
+    for k in ("sound_speed", "density", "alpha_coeff", "BonA"):
+        if k in medium and np.size(medium[k]) > 1:
+            medium[k] = np.pad(np.asarray(medium[k], dtype=np.float64), pad, mode="edge")
+    expanded = {}
+
+    def expand_transducer(tr):
+        if id(tr) not in expanded:
+            t = copy.deepcopy(tr)
+            t.expand_grid(ps)
+            expanded[id(tr)] = t
+        return expanded[id(tr)]
+
+    if isinstance(source, KWaveTransducer):
+        source = expand_transducer(source)
+    else:
+        source = dict(source)
+        if "p0" in source and np.any(np.asarray(source["p0"]) != 0):
+            p0 = np.asarray(source["p0"], dtype=np.float64)
+            if p0.shape != tuple(kgrid.N):
+                raise ValueError("source.p0 must be the same size as the computational grid.")
+            source["p0"] = np.pad(smooth(p0, True) if smooth_p0 else p0, pad)
+        for k in ("p_mask", "u_mask"):
+            if k in source:
+                source[k] = np.pad(np.asarray(source[k]), pad)
+    if isinstance(sensor, KWaveTransducer):
+        sensor = expand_transducer(sensor)
+    else:
+        sensor = dict(sensor)
+        mask = np.asarray(sensor["mask"])
+        if grid_shaped(mask) and not (mask.ndim == 2 and mask.shape[0] == 2 * dim and dim == 3):
+            sensor["mask"] = np.pad(mask, pad)
+        elif mask.ndim == 2 and mask.shape[0] == 2 * dim:
+            sh = np.asarray([int(p) for p in ps] * 2)[:, None]
+            sensor["mask"] = np.asarray(mask, dtype=np.int64) + sh
+    return big, medium, source, sensor, trim
+
+
 def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_size=None,
             pml_alpha=None, pml_inside=True, smooth_p0=True, data_cast="single", cart_interp="nearest"):
     """Build the datasets of the HDF5 input file (saveToDisk.m:44-378)
@@ -74,18 +132,28 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
     Returns (inp, record, start_index, meta)."""
     if cart_interp not in ("nearest", "linear"):
         raise ValueError("cart_interp must be 'nearest' or 'linear'")
-    if not pml_inside:
-        raise NotImplementedError("PMLInside = false is not supported")
     dim = kgrid.dim
-    shape = kgrid.N
     if kgrid.dt is None or kgrid.Nt is None:
         kgrid.make_time(medium["sound_speed"])
     size_def, alpha_def = PML_DEFAULT[dim]
     ps = np.broadcast_to(np.asarray(size_def if pml_size is None else pml_size, dtype=int), (dim,))
     pa = np.broadcast_to(np.asarray(alpha_def if pml_alpha is None else pml_alpha, dtype=float), (dim,))
-    source = dict(source)
+    trim = None
+    if not pml_inside:
+        kgrid, medium, source, sensor, trim = _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0)
+        smooth_p0 = False  # smoothed on the user's grid, before the expansion
+    shape = kgrid.N
+    # a transducer replaces the source struct, or serves as the sensor:
+    # pressure at its active grid points, averaged per element afterwards
+    # (kspaceFirstOrder3DC.m:780-783)
+    tr_source = source if isinstance(source, KWaveTransducer) else None
+    tr_sensor = sensor if isinstance(sensor, KWaveTransducer) else None
+    source = {} if tr_source is not None else dict(source)
+    if tr_sensor is not None:
+        sensor = {"mask": tr_sensor.active_elements_mask, "record_start_index": tr_sensor.record_start_index}
     sensor = dict(sensor)
-    meta = {"dim": dim, "time_rev": False, "cuboid": False, "reorder_index": None}
+    meta = {"dim": dim, "time_rev": False, "cuboid": False, "reorder_index": None, "transducer": tr_sensor,
+            "trim": trim}
 
     # time reversal -> dirichlet pressure source (kspaceFirstOrder3DC.m:437-459)
     if "time_reversal_boundary_data" in sensor:
@@ -183,6 +251,10 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         if "u_frequency_ref" in source:
             mode = "additive-no-correction"
         inp.update(u_source_mode=MODE[mode], u_source_many=many, u_source_index=pos)
+    if tr_source is not None:
+        if dim != 3:
+            raise ValueError("Transducer inputs are only compatible with 3D simulations.")
+        inp.update(transducer_source_datasets(tr_source, c0, kgrid))
 
     # sensor (inputChecking.m:502-634, 1606-1659; 3DC.m:425-431)
     mask = np.asarray(sensor["mask"])
@@ -286,6 +358,10 @@ def postprocess(out: dict, inp: dict, meta: dict):
     (kspaceFirstOrder_saveIntensity.m:42-75, _reorderCartData.m,
     _reorderCuboidCorners.m:33-272)."""
     dim = meta["dim"]
+    if meta.get("trim") is not None:
+        for k in list(out):
+            if k.endswith("_all") or k.endswith("_final"):
+                out[k] = out[k][meta["trim"]]
     if meta.get("interp") is not None:
         _interpolate_sensors(out, meta, dim)
     if meta.get("intensity"):
@@ -323,6 +399,8 @@ def postprocess(out: dict, inp: dict, meta: dict):
             res.append(item)
             start += n
         return res
+    if meta.get("transducer") is not None:
+        out["p"] = meta["transducer"].combine_sensor_data(out["p"])
     if meta["time_rev"]:
         return out["p_final"]
     if not meta["has_record"]:

@@ -225,12 +225,26 @@ def _cosine_series(n, N, coeffs):
 
 
 def get_win_1d(N, kind="Blackman", param=None, symmetric=True):
-    """getWin.m for 1D Blackman and Tukey windows."""
+    """getWin.m for 1D windows: Blackman, Tukey, Rectangular, Hanning,
+    Hamming, Gaussian, Bartlett, Triangular and Cosine (getWin.m:203-247)."""
     N = int(N) + (0 if symmetric else 1)
     n = np.arange(N, dtype=np.float64)
     if kind == "Blackman":
         a = 0.16 if param is None else param
         win = _cosine_series(n, N, [(1 - a) / 2, 0.5, a / 2])
+    elif kind == "Hanning":
+        win = 0.5 - 0.5 * np.cos(2 * np.pi * n / (N - 1))
+    elif kind == "Hamming":
+        win = 0.54 - 0.46 * np.cos(2 * np.pi * n / (N - 1))
+    elif kind == "Gaussian":
+        g = 0.5 if param is None else param
+        win = np.exp(-0.5 * ((n - (N - 1) / 2) / (g * (N - 1) / 2)) ** 2)
+    elif kind == "Bartlett":
+        win = 2 / (N - 1) * ((N - 1) / 2 - np.abs(n - (N - 1) / 2))
+    elif kind == "Triangular":
+        win = 2 / N * (N / 2 - np.abs(n - (N - 1) / 2))
+    elif kind == "Cosine":
+        win = np.cos(np.pi * n / (N - 1) - np.pi / 2)
     elif kind == "Tukey":
         r = 0.5 if param is None else param
         win = np.ones(N)

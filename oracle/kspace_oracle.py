@@ -254,6 +254,17 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
                 u_sig.append(s.reshape(-1, s.shape[-1]).astype(rdt))
             else:
                 u_sig.append(None)
+    # transducer source (kspaceFirstOrder_inputChecking.m:1155-1213): one
+    # signal, a 1-based delay per point, optional apodization weights
+    tr_flag = int(inp.get("transducer_source_flag", 0))
+    if tr_flag:
+        tr_idx = np.asarray(inp["u_source_index"], dtype=np.int64).ravel() - 1
+        tr_sig = np.asarray(inp["transducer_source_input"], dtype=np.float64).ravel().astype(rdt)
+        tr_delay = np.asarray(inp["delay_mask"], dtype=np.int64).ravel()
+        apod = inp.get("transducer_source_apodization")
+        tr_apod = rdt(1) if apod is None else np.asarray(apod, dtype=np.float64).ravel().astype(rdt)
+        if tr_delay.min() < 1 or tr_delay.max() - 1 + tr_flag > tr_sig.size:
+            raise ValueError("delay_mask reads past the end of transducer_source_input")
     p0_flag = int(inp.get("p0_source_flag", 0)) != 0
     if p0_flag:
         p0 = np.asarray(inp["p0_source_input"], dtype=np.float64).reshape(nd, order="F").astype(rdt)
@@ -326,6 +337,10 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
                     u[i] = u[i] + sm
                 else:
                     u[i] = scatter_add(u[i], u_idx, v)
+        # transducer source (kspaceFirstOrder3D.m:886-902): delay_mask advances
+        # by one each step, so step t_index reads sample delay_mask + t_index - 1
+        if tr_flag >= t_index:
+            u[0] = scatter_add(u[0], tr_idx, tr_apod * tr_sig[tr_delay - 1 + t])
         # velocity divergence (kspaceFirstOrder3D.m:905-907)
         du = [rifftn(ddk_neg[i] * (kappa * fftn(u[i]))) for i in range(dim)]
         # mass conservation (kspaceFirstOrder3D.m:910-925)

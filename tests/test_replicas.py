@@ -29,7 +29,7 @@ def _rank(rank, world, port, results):
 
 def test_two_replicas_use_max_time_and_sum_of_units():
     port = 29500 + os.getpid() % 1000
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         results = m.dict()
         mp.start_processes(_rank, args=(2, port, results), nprocs=2, join=True, start_method="spawn")
         res = dict(results)
