@@ -94,6 +94,35 @@ __device__ __forceinline__ void dft5(float2* v) {
   v[3] = c_sub(a2, r2);
 }
 
+// 7-point: the symmetric / antisymmetric pair sums of samples n and 7 - n,
+// X[k] = a_k -+ i b_k and X[7 - k] = a_k +- i b_k for k = 1..3, with
+// a_k = x0 + sum_m cos(2 pi m k / 7) t_m and b_k = sum_m sin(2 pi m k / 7) d_m.
+template <bool INV>
+__device__ __forceinline__ void dft7(float2* v) {
+  const float c1 = 0.623489801858733530525004884004239811f;   // cos(2 pi / 7)
+  const float c2 = -0.222520933956314404288902564496794759f;  // cos(4 pi / 7)
+  const float c3 = -0.900968867902419126236102319507445051f;  // cos(6 pi / 7)
+  const float s1 = 0.781831482468029808708444526674057750f;   // sin(2 pi / 7)
+  const float s2 = 0.974927912181823607018131682993931217f;   // sin(4 pi / 7)
+  const float s3 = 0.433883739117558120475768332848358754f;   // sin(6 pi / 7)
+  const float2 t1 = c_add(v[1], v[6]), t2 = c_add(v[2], v[5]), t3 = c_add(v[3], v[4]);
+  const float2 d1 = c_sub(v[1], v[6]), d2 = c_sub(v[2], v[5]), d3 = c_sub(v[3], v[4]);
+  const float2 x0 = v[0];
+  const float ca[3][3] = {{c1, c2, c3}, {c2, c3, c1}, {c3, c1, c2}};
+  const float sb[3][3] = {{s1, s2, s3}, {s2, -s3, -s1}, {s3, -s1, s2}};
+  v[0] = c_add(x0, c_add(t1, c_add(t2, t3)));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float2 a = make_float2(x0.x + ca[k][0] * t1.x + ca[k][1] * t2.x + ca[k][2] * t3.x,
+                                 x0.y + ca[k][0] * t1.y + ca[k][1] * t2.y + ca[k][2] * t3.y);
+    const float2 b = make_float2(sb[k][0] * d1.x + sb[k][1] * d2.x + sb[k][2] * d3.x,
+                                 sb[k][0] * d1.y + sb[k][1] * d2.y + sb[k][2] * d3.y);
+    const float2 r = c_rot<INV>(b);
+    v[k + 1] = c_add(a, r);
+    v[6 - k] = c_sub(a, r);
+  }
+}
+
 // 8-point: two 4-point transforms of the even / odd samples, then one
 // radix-2 layer with W8^k.
 template <bool INV>
@@ -155,6 +184,8 @@ __device__ __forceinline__ void dft(float2* v) {
     dft4<INV>(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 5) {
     dft5<INV>(v);
+  } else if constexpr (R == 7) {
+    dft7<INV>(v);
   } else if constexpr (R == 8) {
     dft8<INV>(v);
   } else if constexpr (R == 16) {
@@ -228,6 +259,7 @@ __device__ float2* fft_lines(float2* a, float2* b, const float2* __restrict__ tw
       case 2: fft_stage<2, INV, LINE_FAST>(a, b, tw, plan.n, ns, nlines, lay); break;
       case 5: fft_stage<5, INV, LINE_FAST>(a, b, tw, plan.n, ns, nlines, lay); break;
       case 3: fft_stage<3, INV, LINE_FAST>(a, b, tw, plan.n, ns, nlines, lay); break;
+      case 7: fft_stage<7, INV, LINE_FAST>(a, b, tw, plan.n, ns, nlines, lay); break;
       default: break;
     }
     __syncthreads();
@@ -239,16 +271,16 @@ __device__ float2* fft_lines(float2* a, float2* b, const float2* __restrict__ tw
   return a;
 }
 
-// Host-side plan construction: radix-16 stages first, then 8/4/2, then 5, 3.
-// Returns false when n has a prime factor other than 2, 3 or 5.
+// Host-side plan construction: radix-16 stages first, then 8/4/2, then 7, 5, 3.
+// Returns false when n has a prime factor other than 2, 3, 5 or 7.
 inline bool make_fft_plan(int n, FFTPlan* p) {
   p->n = n;
   p->nst = 0;
   int m = n;
   if (n < 1) return false;
   while (m % 16 == 0) { p->rad[p->nst++] = 16; m /= 16; }
-  const int rs[5] = {8, 4, 2, 5, 3};
-  for (int i = 0; i < 5; ++i) {
+  const int rs[6] = {8, 4, 2, 7, 5, 3};
+  for (int i = 0; i < 6; ++i) {
     while (m % rs[i] == 0) {
       if (p->nst >= KWB_MAX_STAGES) return false;
       p->rad[p->nst++] = rs[i];

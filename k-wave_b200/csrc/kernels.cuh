@@ -74,17 +74,10 @@ struct SparseSource {
   int nrows_sig;     // rows in the signal matrix (1 or n)
   int len;           // number of signal samples (active while t <= len)
   int mode;          // 0 dirichlet (set), 1 additive without correction (add)
-};
-
-// Transducer source (kspaceFirstOrder3D.m:886-902): while t <= len, the x
-// velocity at each source point gains apod * sig[delay + t - 1].
-struct TransducerSource {
-  int n;              // source points (0: none)
-  const int* idx;     // sorted linear indices
-  const int* delay;   // 0-based offset into sig of each sorted entry at t = 1
-  const float* apod;  // weight of each sorted entry (nullptr: 1)
-  const float* sig;   // the one input signal
-  int len;            // number of steps the source is active
+  // transducer sources (kspaceFirstOrder3D.m:886-902): one signal read at a
+  // per-entry offset, sample delay + t - 1, times a per-entry weight
+  const int* delay;    // nullptr: no offset
+  const float* weight; // nullptr: 1
 };
 
 // Dense additive source field, added inside the update epilogue while
@@ -148,7 +141,6 @@ struct UArgs {
   SparseSource src;    // velocity sources share one index list ...
   const float* src_sig[3];  // ... with one signal matrix per component
   int src_len[3];
-  TransducerSource tr;  // added to the x component
   DenseSource dsrc[3];
   Sensor sens[3];
   Clock clk;

@@ -386,7 +386,9 @@ static __device__ void sensor_sparse_tile(const Sensor& s, int fi, const float2*
 
 __device__ __forceinline__ float src_value(const SparseSource& s, const float* sig, int j, int t) {
   const int row = (s.nrows_sig == 1) ? 0 : __ldg(s.slot + j);
-  return __ldg(sig + (long long)(t - 1) * s.nrows_sig + row);
+  const int off = s.delay ? __ldg(s.delay + j) : 0;
+  const float v = __ldg(sig + (long long)(t - 1 + off) * s.nrows_sig + row);
+  return s.weight ? __ldg(s.weight + j) * v : v;
 }
 
 template <int NC>
@@ -538,7 +540,8 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
     }
   }
   __syncthreads();
-  // sparse velocity sources (dirichlet / additive without correction)
+  // sparse velocity sources (dirichlet / additive without correction; a
+  // transducer is an additive x source with per-point delays and weights)
   const float* ssig = a.src_sig[ax];
   if (a.src.n > 0 && ssig && t <= a.src_len[ax] && !a.init) {
     const long long rend = min(r0 + 2LL * L, d.row1);
@@ -550,20 +553,6 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
       const float v = src_value(a.src, ssig, j, t);
       const float cur = get_comp(G, lay, q, x);
       set_comp(G, lay, q, x, a.src.mode == 0 ? v : cur + v);
-    }
-    __syncthreads();
-  }
-  // transducer source, after the velocity sources as in the reference loop
-  if (ax == 0 && a.tr.n > 0 && t <= a.tr.len && !a.init) {
-    const long long rend = min(r0 + 2LL * L, d.row1);
-    tile_range(a.tr.idx, a.tr.n, r0 * nx, rend * nx, sh);
-    const int lo = sh[0], hi = sh[1];
-    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      const long long local = (long long)__ldg(a.tr.idx + j) - r0 * nx;
-      const int q = (int)(local / nx), x = (int)(local - (long long)q * nx);
-      const float w = a.tr.apod ? __ldg(a.tr.apod + j) : 1.f;
-      const float v = w * __ldg(a.tr.sig + __ldg(a.tr.delay + j) + (t - 1));
-      set_comp(G, lay, q, x, get_comp(G, lay, q, x) + v);
     }
     __syncthreads();
   }

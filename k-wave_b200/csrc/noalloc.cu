@@ -227,7 +227,7 @@ extern "C" int kw_kspace_gradient_noalloc(const float* d_f, float* d_gx, float* 
                 (unsigned long long)nx, (unsigned long long)ny, MAX_EDGE);
   GradArgs a{};
   if (!make_fft_plan((int)nx, &a.px) || !make_fft_plan((int)ny, &a.py))
-    return fail(status, KW_ERR_UNSUPPORTED, "grid edges must be products of 2, 3 and 5 (got %llu x %llu)",
+    return fail(status, KW_ERR_UNSUPPORTED, "grid edges must be products of 2, 3, 5 and 7 (got %llu x %llu)",
                 (unsigned long long)nx, (unsigned long long)ny);
   if (!(dx > 0.f) || !(dy > 0.f) || !(dt > 0.f) || !(c_ref >= 0.f) || !std::isfinite(dx) || !std::isfinite(dy) ||
       !std::isfinite(dt) || !std::isfinite(c_ref))

@@ -143,9 +143,9 @@ static double db2neper(double a, double y) {
   return 100.0 * a * std::pow(1e-6 / (2 * M_PI), y) / (20.0 * std::log10(std::exp(1.0)));
 }
 
-static bool factors_235(uint64_t n) {
+static bool factors_2357(uint64_t n) {
   if (n == 0) return false;
-  for (uint64_t p : {2ull, 3ull, 5ull})
+  for (uint64_t p : {2ull, 3ull, 5ull, 7ull})
     while (n % p == 0) n /= p;
   return n == 1;
 }
@@ -230,8 +230,8 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
   if (in->Ny == 1) throw KwError(KW_ERR_UNSUPPORTED, "1D simulations are not supported (Ny must be > 1)");
   for (uint64_t n : {in->Nx, in->Ny, in->Nz}) {
-    if (n > 1 && !factors_235(n))
-      throw KwError(KW_ERR_UNSUPPORTED, "grid sizes must factor into 2, 3 and 5");
+    if (n > 1 && !factors_2357(n))
+      throw KwError(KW_ERR_UNSUPPORTED, "grid sizes must factor into 2, 3, 5 and 7");
     if (n > 4096) throw KwError(KW_ERR_UNSUPPORTED, "grid sizes above 4096 are not supported");
   }
   if (in->Nx < 2) throw KwError(KW_ERR_UNSUPPORTED, "Nx must be at least 2");
@@ -570,7 +570,6 @@ void Session::setup_sources(const kw_input* in) {
   }
   // transducer source (kspaceFirstOrder_inputChecking.m:1155-1213 builds
   // what the file holds; kspaceFirstOrder3D.m:886-902 applies it)
-  tsrc = TransducerSource{};
   if (in->transducer_source_flag) {
     if (d.dim != 3) throw KwError(KW_ERR_INVALID_ARGUMENT, "transducer sources are 3D only");
     if (uf[0] || uf[1] || uf[2])
@@ -596,12 +595,21 @@ void Session::setup_sources(const kw_input* in) {
       dl[j] = (int)(dm - 1);
       if (!ap.empty()) ap[j] = in->transducer_source_apodization[sl[j]];
     }
-    tsrc.n = (int)si.size();
-    tsrc.idx = up(tsrc_idx, si.data(), si.size(), st);
-    tsrc.delay = up(tsrc_delay, dl.data(), dl.size(), st);
-    tsrc.apod = ap.empty() ? nullptr : up(tsrc_apod, ap.data(), ap.size(), st);
-    tsrc.sig = up(tsrc_sig, in->transducer_source_input, nsig, st);
-    tsrc.len = (int)len;
+    // an additive x-velocity source whose entries read one signal at their
+    // own offsets (SparseSource::delay, ::weight)
+    u_nsrc = (int)si.size();
+    u_nsig = 1;
+    u_mode = 1;
+    usrc.n = u_nsrc;
+    usrc.idx = up(usrc_idx, si.data(), si.size(), st);
+    usrc.slot = nullptr;
+    usrc.nrows_sig = 1;
+    usrc.mode = 1;
+    usrc.len = 0;
+    usrc.delay = up(tsrc_delay, dl.data(), dl.size(), st);
+    usrc.weight = ap.empty() ? nullptr : up(tsrc_apod, ap.data(), ap.size(), st);
+    usig_d[0] = up(usig_buf[0], in->transducer_source_input, nsig, st);
+    u_len[0] = (int)len;
   }
 }
 
@@ -930,7 +938,6 @@ UArgs Session::u_args(float2* const* S) {
   ua.init = 0;
   ua.do_r2c = 1;
   ua.src = usrc;
-  ua.tr = tsrc;
   ua.clk = clk;
   return ua;
 }

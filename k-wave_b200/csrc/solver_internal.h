@@ -120,8 +120,7 @@ class Session {
   DenseSource pdense{}, udense[3]{};
   DevBuf psrc_idx, psrc_slot, psrc_sig, psrc_field;
   DevBuf usrc_idx, usrc_slot, usig_buf[3], ufield_buf[3], ones_buf;
-  TransducerSource tsrc{};
-  DevBuf tsrc_idx, tsrc_delay, tsrc_apod, tsrc_sig;
+  DevBuf tsrc_delay, tsrc_apod;
   const float* usig_d[3]{};
   int u_len[3]{};
   int p_mode = 0, p_len = 0, p_nsrc = 0, p_nsig = 1;

@@ -102,7 +102,7 @@ def test_invalid_inputs_fail_on_the_host():
 
     inp, record, start, _ = case_2d_p0()
     bad = dict(inp)
-    bad["Nx"] = 7 * 8  # a prime factor of 7
+    bad["Nx"] = 11 * 8  # a prime factor above 7
     with pytest.raises(_lib.KwaveError) as e:
         _lib.solve(bad, record)
     assert e.value.code == 5  # KW_ERR_UNSUPPORTED

@@ -143,8 +143,8 @@ def test_output_sizes_and_errors():
     with pytest.raises(_lib.KwaveError):
         _solve(bad, record)
     bad = dict(inp)
-    bad["Nx"] = 7 * 8
-    with pytest.raises(_lib.KwaveError):
+    bad["Nx"] = 11 * 8  # a prime factor above 7
+    with pytest.raises(_lib.KwaveError, match="factor"):
         _solve(bad, record)
 
 
@@ -189,6 +189,18 @@ def test_2d_compile_time_mixed_radix_sizes(n):
 @pytest.mark.parametrize("n", [(72, 75, 80), (81, 90, 64)])
 def test_3d_compile_time_mixed_radix_sizes(n):
     inp, record, start, _ = case_3d_het(n=n, nt=24, record=("p", "p_rms", "u"))
+    _check(inp, record, TOL)
+
+
+@pytest.mark.parametrize("n", [(56, 42), (112, 49), (98, 70)])
+def test_2d_radix7_sizes(n):
+    """Edges with a factor 7 (the runtime FFT engine's radix-7 stage)."""
+    inp, record, start, _ = case_2d_p0(n=n, nt=30, record=("p", "p_max", "u", "p_final"))
+    _check(inp, record, TOL_LOSSLESS)
+
+
+def test_3d_radix7_sizes():
+    inp, record, start, _ = case_3d_het(n=(28, 36, 35), nt=24, record=("p", "p_rms", "u", "p_final"))
     _check(inp, record, TOL)
 
 

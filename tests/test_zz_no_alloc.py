@@ -97,7 +97,7 @@ def test_gradient_noalloc_rejects_what_it_cannot_hold():
         _lib.kspace_gradient_noalloc(d.data_ptr(), d.data_ptr(), None, 2048, 4, *args)
     assert e.value.code == _lib.KW_ERR_INVALID_ARGUMENT and "1024" in str(e.value)
     with pytest.raises(_lib.KwaveError) as e:
-        _lib.kspace_gradient_noalloc(d.data_ptr(), d.data_ptr(), None, 4, 7, *args)
+        _lib.kspace_gradient_noalloc(d.data_ptr(), d.data_ptr(), None, 4, 11, *args)
     assert e.value.code == _lib.KW_ERR_UNSUPPORTED
     host = np.zeros(16, np.float32)
     with pytest.raises(_lib.KwaveError) as e:
