@@ -401,8 +401,8 @@ __device__ __forceinline__ int row_lines(int L) {
 // streams everything the tile will read while the block is still in its
 // first phase; the later loads then hit L2.  Bulk prefetches need 16-byte
 // aligned addresses and sizes: real fields with nx % 4 == 0 and half-spectrum
-// rows rounded up to an even number of bins (the pitch nxp is a multiple of
-// 32 bins, so the rounded row stays inside it).
+// rows rounded up to an even number of bins (the pitch nxp is that even
+// count, so the rounded row stays inside it).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");

@@ -299,10 +299,15 @@ bool tma_supported(int n) { return n == 64 || n == 128 || n == 256; }
 
 // Tensor map over a half-spectrum buffer [nz][ny][nxp] (8-byte elements),
 // box {lines, ny or 1, 1 or nz} for transforms along y (yaxis 1) or z (2).
+// The x extent is the nxh bins in use, not the pitch: the last column tile
+// of a row is loaded with zeros past bin nxh - 1 and stored clipped there,
+// so padding costs no memory traffic.  Tiles start at x = cx * lines, a
+// multiple of 16 bytes.
 bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n) {
   if (!get_encoder()) return false;
   const int lines = ct_lines_of(n);
-  cuuint64_t dims[3] = {(cuuint64_t)d.nxp, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
+  if (d.nxp % 2 != 0 || (lines * 8) % 16 != 0) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)d.nxh, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
   cuuint64_t strides[2] = {(cuuint64_t)d.nxp * 8, (cuuint64_t)d.nxp * d.ny * 8};
   cuuint32_t box[3] = {(cuuint32_t)lines, yaxis == 1 ? (cuuint32_t)d.ny : 1u, yaxis == 2 ? (cuuint32_t)d.nz : 1u};
   cuuint32_t es[3] = {1, 1, 1};

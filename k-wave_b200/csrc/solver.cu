@@ -240,7 +240,11 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   d.nz = (int)in->Nz;
   d.dim = (in->Nz == 1) ? 2 : 3;
   d.nxh = d.nx / 2 + 1;
-  d.nxp = (d.nxh + 31) / 32 * 32;  // whole TMA column tiles: no box leaves the buffer
+  // row pitch in bins: even, so rows start on 16-byte boundaries (TMA strides,
+  // paired-bin vector accesses); TMA column tiles that run past bin nxh - 1
+  // are cut by the tensor maps' extent (zero fill on loads, clipped stores), so
+  // no padding bin is read from or written to memory
+  d.nxp = (d.nxh + 1) / 2 * 2;
   d.nrows = (long long)d.ny * d.nz;
   d.npts = (long long)d.nx * d.nrows;
   d.row0 = 0;
@@ -1320,7 +1324,7 @@ Session::~Session() {
 size_t Session::device_bytes_estimate(const kw_input* in, const kw_options* o) {
   const size_t n = (size_t)(in->Nx * in->Ny * in->Nz);
   const size_t dim = in->Nz == 1 ? 2 : 3;
-  const size_t nxp = ((in->Nx / 2 + 1) + 31) / 32 * 32;
+  const size_t nxp = ((in->Nx / 2 + 1) + 1) / 2 * 2;
   size_t b = 4 * 8 * nxp * in->Ny * in->Nz + 2 * dim * 4 * n;  // spectra, u, rho
   b += 4 * n * (2 + dim);                                       // medium maps
   return b;
