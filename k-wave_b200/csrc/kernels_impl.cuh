@@ -33,6 +33,12 @@ struct Tile {
 };
 // Row (x) tiles use half as many lines: smaller blocks, more of them per SM,
 // so their load / transform / store phases overlap.
+// The row kernels' 4-wide epilogue loops and their spectrum load / store
+// loops run without unrolling: at 256 points per row this cut registers
+// (k_x_rho 118 -> 90, k_x_u 72 -> 64) and instruction-fetch stalls, and the
+// 256^3 step went from 1.43 to 1.36 ms against unroll factors of 2-4.
+constexpr int kRowLoopUnroll = 1;
+
 template <int NC>
 struct RTile {
   static constexpr int LINES = NC > 0 ? (ct_lines_of(NC) / 2 > 0 ? ct_lines_of(NC) / 2 : 1) : 0;
@@ -168,7 +174,7 @@ __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* b
     // paired 16-byte loads; each loaded bin k also fills its mirror n - k
     constexpr int n = NC, np = NC / 4 + 1;  // bin pairs (k, k+1), k even, k <= n/2
     const int total = L * np;
-#pragma unroll 4
+#pragma unroll (kRowLoopUnroll)
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int l = i / np, k = 2 * (i - l * np);
       const long long ra = r0 + 2 * l, rb = ra + 1;
@@ -234,7 +240,7 @@ __device__ __forceinline__ void store_r2c(const float2* buf, float2* __restrict_
   if constexpr (NC > 0 && NC % 4 == 0) {
     constexpr int n = NC, nh = NC / 2 + 1, np = NC / 4 + 1;
     const int total = L * np;
-#pragma unroll 4
+#pragma unroll (kRowLoopUnroll)
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int l = i / np, k = 2 * (i - l * np);
       const long long ra = r0 + 2 * l, rb = ra + 1;
@@ -480,7 +486,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   constexpr bool VEC = NC > 0 && NC % 4 == 0;
   if constexpr (VEC) {
     // 4 consecutive points per iteration, 16-byte global accesses
-#pragma unroll 4
+#pragma unroll (kRowLoopUnroll)
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
@@ -558,7 +564,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   }
   const Sensor& s = a.sens[ax];
   if constexpr (VEC) {
-#pragma unroll 4
+#pragma unroll (kRowLoopUnroll)
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
@@ -667,7 +673,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
   constexpr bool VEC = NC > 0 && NC % 4 == 0;
   if (VEC && !sp) {
     // 4 consecutive points per iteration, 16-byte global accesses
-#pragma unroll 2
+#pragma unroll (kRowLoopUnroll)
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
@@ -892,7 +898,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
   }
   const int total = 2 * L * nx;
   if constexpr (NC > 0 && NC % 4 == 0) {
-#pragma unroll 4
+#pragma unroll (kRowLoopUnroll)
     for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
       const int q = i / nx, x = i - q * nx;
       const long long row = r0 + q;
