@@ -83,7 +83,7 @@ void read_input(const std::string& path, InputFile& F) {
   h5::Reader r(path);
   const std::string ft = r.attribute_string("/", "file_type");
   if (!ft.empty() && ft != "input") throw IoError(KW_ERR_IO, path + " is a '" + ft + "' file, not an input file");
-  for (const char* unsupported : {"elastic_flag", "axisymmetric_flag", "nonuniform_grid_flag"})
+  for (const char* unsupported : {"elastic_flag", "nonuniform_grid_flag"})
     if (opt_u64(r, unsupported, 0) != 0)
       throw IoError(KW_ERR_UNSUPPORTED, std::string(unsupported) + " is set: only the fluid solver is supported");
   for (const char* sflag : {"sxx_source_flag", "syy_source_flag", "szz_source_flag", "sxy_source_flag",
@@ -154,6 +154,7 @@ void read_input(const std::string& path, InputFile& F) {
     if (in.uy_source_flag) { need(r, "uy_source_input"); in.uy_source_input = F.keep_f(r.read_float("/uy_source_input")); }
     if (in.uz_source_flag) { need(r, "uz_source_input"); in.uz_source_input = F.keep_f(r.read_float("/uz_source_input")); }
   }
+  in.axisymmetric_flag = opt_u64(r, "axisymmetric_flag", 0);
   in.transducer_source_flag = opt_u64(r, "transducer_source_flag", 0);
   if (in.transducer_source_flag) {
     for (const char* n : {"u_source_index", "delay_mask", "transducer_source_input"}) need(r, n);

@@ -31,6 +31,7 @@ enum SpecOpKind {
   OP_IDENTITY = 5,
   OP_KAPPA = 6,      // kappa alone (the axis factor applied elsewhere)
   OP_SHIFT_NEG = 7,  // exp(-i k_a d_a / 2): staggered -> regular grid along axis a, no kappa
+  OP_KAPPA_SHIFT_NEG = 8,  // kappa * exp(-i k_a d_a / 2): the axisymmetric u_r / r term
 };
 
 struct SpecOp {
@@ -166,6 +167,7 @@ struct RhoArgs {
   float2* S_p;         // lossless / stokes: x-transform of p
   Sensor sens;
   Clock clk;
+  const float2* S_rr;  // axisymmetric: the u_r / r spectrum, added to S[1] as it is read
 };
 
 struct EosArgs {

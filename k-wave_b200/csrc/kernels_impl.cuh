@@ -169,7 +169,8 @@ __device__ __forceinline__ void set_comp(float2* b, RowLayout lay, int q, int x,
 // which is the Hermitian projection that real(ifftn(.)) performs.
 template <int NC>
 __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* buf, RowLayout lay, const Dims& d,
-                                         long long r0, int L, const float2* __restrict__ kmul = nullptr) {
+                                         long long r0, int L, const float2* __restrict__ kmul = nullptr,
+                                         const float2* __restrict__ S2 = nullptr) {
   if constexpr (NC > 0 && NC % 4 == 0) {
     // paired 16-byte loads; each loaded bin k also fills its mirror n - k
     constexpr int n = NC, np = NC / 4 + 1;  // bin pairs (k, k+1), k even, k <= n/2
@@ -181,6 +182,13 @@ __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* b
       float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
       if (ra < d.row1) A = *reinterpret_cast<const float4*>(S + ra * d.nxp + k);
       if (rb < d.row1) B = *reinterpret_cast<const float4*>(S + rb * d.nxp + k);
+      if (S2) {
+        float4 A2 = make_float4(0.f, 0.f, 0.f, 0.f), B2 = A2;
+        if (ra < d.row1) A2 = *reinterpret_cast<const float4*>(S2 + ra * d.nxp + k);
+        if (rb < d.row1) B2 = *reinterpret_cast<const float4*>(S2 + rb * d.nxp + k);
+        A = make_float4(A.x + A2.x, A.y + A2.y, A.z + A2.z, A.w + A2.w);
+        B = make_float4(B.x + B2.x, B.y + B2.y, B.z + B2.z, B.w + B2.w);
+      }
       if (kmul) {
         const float2 m0 = __ldg(kmul + k), m1 = __ldg(kmul + min(k + 1, n / 2));
         float2 t = c_mul(make_float2(A.x, A.y), m0), u = c_mul(make_float2(A.z, A.w), m1);
@@ -216,6 +224,10 @@ __device__ __forceinline__ void load_c2r(const float2* __restrict__ S, float2* b
     float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
     if (ra < d.row1) A = S[ra * d.nxp + kk];
     if (rb < d.row1) B = S[rb * d.nxp + kk];
+    if (S2) {
+      if (ra < d.row1) A = c_add(A, S2[ra * d.nxp + kk]);
+      if (rb < d.row1) B = c_add(B, S2[rb * d.nxp + kk]);
+    }
     if (kmul) {
       const float2 m = __ldg(kmul + kk);
       A = c_mul(A, m);
@@ -625,7 +637,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
   if constexpr (CT) {
 #pragma unroll 1
     for (int f = 0; f < dim; ++f) {
-      load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L);
+      load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L, nullptr, f == 1 ? a.S_rr : nullptr);
       __syncthreads();
       if constexpr (NC % 4 == 0) {  // what the next phase reads streams in during this FFT
         TilePrefetch pf(d, r0, L);
@@ -655,7 +667,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
             ib = b;
         }
       }
-      load_c2r<NC>(a.S[f], pool[ia], lay, d, r0, L);
+      load_c2r<NC>(a.S[f], pool[ia], lay, d, r0, L, nullptr, f == 1 ? a.S_rr : nullptr);
       __syncthreads();
       D[f] = tile_fft<NC, true, false>(pool[ia], pool[ib], tw, plan, L, lay);
       used[(D[f] == pool[ia]) ? ia : ib] = true;

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
           } else {
             const float2* tab = (op.kind == OP_GRAD_POS)   ? T.ddk_pos[op.axis]
                                 : (op.kind == OP_GRAD_NEG) ? T.ddk_neg[op.axis]
-                                                           : T.shift_neg[op.axis];
+                                                           : T.shift_neg[op.axis];  // shift, kappa * shift
             ev.dconst = __ldg(tab + (op.axis == 0 ? ix : o));
           }
         }
@@ -358,7 +358,8 @@ template <int NC>
 static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   const int kind = a.op[0].kind;
   const bool one = a.fanout == 1;
-  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA || kind == OP_SHIFT_NEG)
+  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA || kind == OP_SHIFT_NEG ||
+      kind == OP_KAPPA_SHIFT_NEG)
     return one ? fused_tma_t<NC, FC_GRAD, true>(a, tw, T, st) : fused_tma_t<NC, FC_GRAD, false>(a, tw, T, st);
   if (kind == OP_NABLA1 || kind == OP_NABLA2)
     return one ? fused_tma_t<NC, FC_NABLA, true>(a, tw, T, st) : fused_tma_t<NC, FC_NABLA, false>(a, tw, T, st);

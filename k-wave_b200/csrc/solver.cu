@@ -47,9 +47,11 @@ cudaError_t launch_x_r2c(const float* f, float2* S, const Dims& d, const FFTPlan
 cudaError_t launch_x_c2r(const float2* S, float* out, int accumulate, const Dims& d, const FFTPlan& plan,
                          const float2* tw, int L, cudaStream_t st);
 cudaError_t launch_scatter(float* f, const int* idx, const int* slot, int n, const float* sig,
-                           int nrows_sig, int t, cudaStream_t st);
+                           int nrows_sig, int t, const float* weight, cudaStream_t st);
 cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim,
                             long long n, cudaStream_t st);
+cudaError_t launch_scale_rows(float* out, const float* in, const float* r, int nx, int ny, long long n,
+                              cudaStream_t st);
 cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& clk, long long n,
                                 cudaStream_t st);
 cudaError_t launch_advance(int* t, cudaStream_t st);
@@ -220,6 +222,92 @@ struct PhaseTimer {
   }
 };
 
+const kw_input* Session::expand_axisymmetric(const kw_input* in) {
+  if (in->Nz != 1) throw KwError(KW_ERR_INVALID_ARGUMENT, "axisymmetric grids are 2D (Nz must be 1)");
+  if (in->absorbing_flag == 1)
+    throw KwError(KW_ERR_UNSUPPORTED, "axisymmetric simulations take Stokes absorption only (absorbing_flag 2)");
+  if (in->ux_source_flag || in->uy_source_flag || in->uz_source_flag || in->transducer_source_flag)
+    throw KwError(KW_ERR_UNSUPPORTED, "velocity and transducer sources are not supported on axisymmetric grids");
+  if (opt.u_non_staggered_raw)
+    throw KwError(KW_ERR_UNSUPPORTED, "u_non_staggered_raw is not supported on axisymmetric grids");
+  if (in->Ny < 2 || in->Nx < 1) throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx and Ny must be positive");
+  const uint64_t nx = in->Nx, ny = in->Ny, ny4 = 4 * ny;
+  // column maps: expanded radial index j -> original column and sign, for the
+  // pressure points (even about the axis, odd about the outer radius, zero on
+  // the outer-radius columns) and the radially staggered points
+  std::vector<uint64_t> pc(ny4), sc(ny4);
+  std::vector<float> ps(ny4), ss(ny4);
+  for (uint64_t j = 0; j < ny4; ++j) {
+    const uint64_t q = j / ny, m = j % ny;
+    if (q == 0 || q == 2) {
+      pc[j] = m;
+      ps[j] = (q == 0) ? 1.f : -1.f;
+    } else {
+      pc[j] = (m == 0) ? ny - 1 : ny - m;  // m == 0: the odd point, zero field; medium from the edge
+      ps[j] = (m == 0) ? 0.f : (q == 1 ? -1.f : 1.f);
+    }
+    sc[j] = (q == 0 || q == 2) ? m : ny - 1 - m;
+    ss[j] = (q < 2) ? 1.f : -1.f;
+  }
+  auto expand = [&](const kw_field& f, bool staggered, std::vector<float>& store) {
+    kw_field o = f;
+    if (f.numel <= 1) return o;
+    if (f.numel != nx * ny) throw KwError(KW_ERR_INVALID_ARGUMENT, "axisymmetric medium arrays must be Nx x Ny");
+    store.resize(nx * ny4);
+    const std::vector<uint64_t>& col = staggered ? sc : pc;
+    for (uint64_t j = 0; j < ny4; ++j)
+      for (uint64_t x = 0; x < nx; ++x) store[x + nx * j] = f.data[x + nx * col[j]];
+    o.data = store.data();
+    o.numel = store.size();
+    return o;
+  };
+  asx.in = *in;
+  asx.in.Ny = ny4;
+  asx.in.c0 = expand(in->c0, false, asx.c0);
+  asx.in.rho0 = expand(in->rho0, false, asx.rho0);
+  asx.in.rho0_sgx = expand(in->rho0_sgx, false, asx.sgx);
+  asx.in.rho0_sgy = expand(in->rho0_sgy, true, asx.sgy);
+  if (in->nonlinear_flag) asx.in.BonA = expand(in->BonA, false, asx.bona);
+  if (in->absorbing_flag) asx.in.alpha_coeff = expand(in->alpha_coeff, false, asx.alpha);
+  if (in->p0_source_flag && in->p0_source_input) {
+    asx.p0.resize(nx * ny4);
+    for (uint64_t j = 0; j < ny4; ++j)
+      for (uint64_t x = 0; x < nx; ++x) asx.p0[x + nx * j] = ps[j] * in->p0_source_input[x + nx * pc[j]];
+    asx.in.p0_source_input = asx.p0.data();
+  }
+  p_rows0 = in->p_source_index_numel;
+  if (in->p_source_flag && in->p_source_index) {
+    // each source point and its mirror images, with the sign of the pressure there
+    for (uint64_t e = 0; e < in->p_source_index_numel; ++e) {
+      const uint64_t lin = in->p_source_index[e];
+      if (lin < 1 || lin > nx * ny) throw KwError(KW_ERR_INVALID_ARGUMENT, "p_source_index holds an index outside the grid");
+      const uint64_t x = (lin - 1) % nx, y = (lin - 1) / nx;
+      const uint64_t cols[4] = {y, 2 * ny - y, 2 * ny + y, 4 * ny - y};
+      const float sg[4] = {1.f, -1.f, -1.f, 1.f};
+      for (int k = 0; k < 4; ++k) {
+        if ((k == 1 || k == 3) && y == 0) continue;
+        asx.p_idx.push_back(x + nx * cols[k] + 1);
+        asx.p_orig.push_back((int)e);
+        asx.p_w.push_back(sg[k]);
+      }
+    }
+    asx.in.p_source_index = asx.p_idx.data();
+    asx.in.p_source_index_numel = asx.p_idx.size();
+  }
+  if (in->sensor_mask_type == 0) {
+    for (uint64_t j = 0; j < in->sensor_mask_index_numel; ++j)
+      if (in->sensor_mask_index[j] < 1 || in->sensor_mask_index[j] > nx * ny)
+        throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_index holds an index outside the grid");
+  } else if (in->sensor_mask_corners) {
+    for (uint64_t k = 0; k + 5 < in->sensor_mask_corners_numel; k += 6)
+      if (in->sensor_mask_corners[k + 4] > ny)
+        throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_corners reach past the grid");
+  }
+  axisym = true;
+  ny0 = (int)ny;
+  return &asx.in;
+}
+
 void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   allow_ring_ = allow_ring;
   if (!in || !o) throw KwError(KW_ERR_INVALID_ARGUMENT, "input and options must not be NULL");
@@ -228,6 +316,8 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   if (opt.start_index == 0) opt.start_index = 1;
   if (in->Nx < 1 || in->Ny < 1 || in->Nz < 1 || in->Nt < 1)
     throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
+  p_rows0 = in->p_source_index_numel;
+  if (in->axisymmetric_flag) in = expand_axisymmetric(in);
   if (in->Ny == 1) throw KwError(KW_ERR_UNSUPPORTED, "1D simulations are not supported (Ny must be > 1)");
   for (uint64_t n : {in->Nx, in->Ny, in->Nz}) {
     if (n > 1 && !factors_2357(n))
@@ -323,9 +413,26 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     T.shift_neg[a] = up(sh_buf[a], sh.data(), cnt, st);
     const uint64_t psz[3] = {in->pml_x_size, in->pml_y_size, in->pml_z_size};
     const double pal[3] = {in->pml_x_alpha, in->pml_y_alpha, in->pml_z_alpha};
-    if (psz[a] * 2 > (uint64_t)ns[a]) throw KwError(KW_ERR_INVALID_ARGUMENT, "PML is larger than the grid");
-    std::vector<double> pm = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], false);
-    std::vector<double> pms = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], true);
+    std::vector<double> pm, pms;
+    if (axisym && a == 1) {
+      // getPML.m with `axisymmetric`: the profile at the outer radius only,
+      // then mirrored like the fields it damps
+      if (psz[a] > (uint64_t)ny0) throw KwError(KW_ERR_INVALID_ARGUMENT, "PML is larger than the grid");
+      std::vector<double> p1 = pml_profile(ny0, dd[a], dt, c_ref, (int)psz[a], pal[a], false);
+      std::vector<double> s1 = pml_profile(ny0, dd[a], dt, c_ref, (int)psz[a], pal[a], true);
+      for (uint64_t j = 0; j < psz[a]; ++j) p1[j] = s1[j] = 1.0;
+      pm.resize(ns[a]);
+      pms.resize(ns[a]);
+      for (int j = 0; j < ns[a]; ++j) {
+        const int q = j / ny0, m = j % ny0;
+        pm[j] = (q == 0 || q == 2) ? p1[m] : p1[m == 0 ? ny0 - 1 : ny0 - m];
+        pms[j] = (q == 0 || q == 2) ? s1[m] : s1[ny0 - 1 - m];
+      }
+    } else {
+      if (psz[a] * 2 > (uint64_t)ns[a]) throw KwError(KW_ERR_INVALID_ARGUMENT, "PML is larger than the grid");
+      pm = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], false);
+      pms = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], true);
+    }
     std::vector<float> f1(pm.begin(), pm.end()), f2(pms.begin(), pms.end());
     pml_d[a] = up(pml_buf[a], f1.data(), f1.size(), st);
     pml_sg_d[a] = up(pmls_buf[a], f2.data(), f2.size(), st);
@@ -416,9 +523,23 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     ck(cudaMemsetAsync(u_buf[a].p, 0, fb, st), "memset");
     ck(cudaMemsetAsync(rho_buf[a].p, 0, fb, st), "memset");
   }
-  for (int s = 0; s < 4; ++s) {
+  const int nspec = axisym ? 5 : 4;
+  for (int s = 0; s < nspec; ++s) {
     S_buf[s].alloc(sb, st);
     ck(cudaMemsetAsync(S_buf[s].p, 0, sb, st), "memset");
+  }
+  if (axisym) {
+    // 1 / r on the radially staggered points, signed as u_r / r is mirrored
+    // (kspaceFirstOrderAS.m:570-571, 920-923): [1/r, -flip(1/r), 1/r, -flip(1/r)]
+    std::vector<float> ir(d.ny);
+    for (int j = 0; j < d.ny; ++j) {
+      const int q = j / ny0, m = j % ny0;
+      const int src = (q == 0 || q == 2) ? m : ny0 - 1 - m;
+      const double r = (src + 0.5) * in->dy;
+      ir[j] = (float)(((q == 0 || q == 2) ? 1.0 : -1.0) / r);
+    }
+    up(inv_r_buf, ir.data(), ir.size(), st);
+    ur_buf.alloc(fb, st);
   }
   err_buf.alloc(sizeof(int), st);
   ck(cudaMemsetAsync(err_buf.p, 0, sizeof(int), st), "memset");
@@ -429,7 +550,7 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   const bool tma_ok = !(no_tma && no_tma[0] == '1');
   use_tma[1] = tma_ok && tma_supported(d.ny);
   use_tma[2] = tma_ok && d.dim == 3 && tma_supported(d.nz);
-  for (int s = 0; s < 4; ++s) {
+  for (int s = 0; s < nspec; ++s) {
     if (use_tma[1] && !make_spec_map(&map_y[s], S_buf[s].p, d, 1, d.ny)) use_tma[1] = false;
     if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;
   }
@@ -477,10 +598,20 @@ void Session::setup_sources(const kw_input* in) {
       throw KwError(KW_ERR_INVALID_ARGUMENT, "p_source_index / p_source_input missing");
     std::vector<int> si, sl;
     sort_indices(in->p_source_index, in->p_source_index_numel, d.npts, si, sl, "p_source_index");
-    const int nsig = in->p_source_many ? (int)in->p_source_index_numel : 1;
+    const int nsig = in->p_source_many ? (int)p_rows0 : 1;
     p_mode = (int)in->p_source_mode;
     if (p_mode < 0 || p_mode > 2) throw KwError(KW_ERR_INVALID_ARGUMENT, "p_source_mode must be 0, 1 or 2");
     p_len = (int)in->p_source_flag;
+    const float* dw = nullptr;
+    if (axisym) {
+      // mirrored entries read their original point's signal, with its sign
+      std::vector<float> w(sl.size());
+      for (size_t j = 0; j < sl.size(); ++j) {
+        w[j] = asx.p_w[sl[j]];
+        sl[j] = asx.p_orig[sl[j]];
+      }
+      dw = up(psrc_w, w.data(), w.size(), st);
+    }
     const int* didx = up(psrc_idx, si.data(), si.size(), st);
     const int* dslot = up(psrc_slot, sl.data(), sl.size(), st);
     const float* dsig = up(psrc_sig, in->p_source_input, (size_t)nsig * p_len, st);
@@ -494,7 +625,7 @@ void Session::setup_sources(const kw_input* in) {
         std::vector<float> ones(1, 1.0f);
         DevBuf onebuf;
         const float* d1 = up(onebuf, ones.data(), 1, st);
-        corrected_source((float*)psrc_field.p, didx, dslot, p_nsrc, d1, 1, 1);
+        corrected_source((float*)psrc_field.p, didx, dslot, p_nsrc, d1, 1, 1, dw);
         ck(cudaStreamSynchronize(st), "source setup");
         pdense.field = (const float*)psrc_field.p;
         pdense.sig = dsig;
@@ -512,6 +643,7 @@ void Session::setup_sources(const kw_input* in) {
       psrc.nrows_sig = nsig;
       psrc.len = p_len;
       psrc.mode = p_mode;  // 0 dirichlet, 1 add
+      psrc.weight = dw;
     }
   }
   usrc = SparseSource{};
@@ -620,9 +752,9 @@ void Session::setup_sources(const kw_input* in) {
 // out = real(ifftn(source_kappa .* fftn(scatter(sig(:, t)))))
 // (kspaceFirstOrder3D.m:813-821, 938-945)
 void Session::corrected_source(float* out, const int* idx, const int* slot, int n, const float* sig,
-                               int nrows_sig, int t) {
+                               int nrows_sig, int t, const float* weight) {
   ck(cudaMemsetAsync(out, 0, sizeof(float) * d.npts, st), "memset");
-  ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, st), "scatter");
+  ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, weight, st), "scatter");
   float2* S = (float2*)S_buf[3].p;
   ck(launch_x_r2c(out, S, d, plan[0], twd[0], rowL, st), "x_r2c");
   run_spectral({3}, {3}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
@@ -1014,16 +1146,31 @@ void Session::enqueue_step_body(uint64_t t) {
       ++launches_;
       col_pass(false, f123, z0, nzs);
     }
+    if (axisym) {
+      // the radial term of the divergence: u_r / r, transformed along x
+      // (kspaceFirstOrderAS.m:920-934)
+      ck(launch_scale_rows((float*)ur_buf.p, (const float*)u_buf[1].p, (const float*)inv_r_buf.p, d.nx, d.ny,
+                           d.npts, st), "u_r / r");
+      ck(launch_x_r2c((const float*)ur_buf.p, (float2*)S_buf[4].p, d, plan[0], twd[0], rowL, st), "x_r2c");
+      launches_ += 2;
+    }
     record_non_staggered();
     // (2) mass conservation: div u -> rho, EOS (:905-1017)
     {
       std::vector<SpecOp> ops;
       for (int a = 0; a < d.dim; ++a) ops.push_back(SpecOp{OP_GRAD_NEG, a});
-      fused_pass(f123, f123, ops, 1);
+      if (axisym) {
+        // the radial divergence gains kappa * shift_neg * F{u_r / r}
+        // (kspaceFirstOrderAS.m:930-931), summed into du_r/dr as x_rho reads it
+        ops.push_back(SpecOp{OP_KAPPA_SHIFT_NEG, 1});
+        fused_pass({1, 2, 4}, {1, 2, 4}, ops, 1);
+      } else {
+        fused_pass(f123, f123, ops, 1);
+      }
     }
     if (p_many_additive && (int)t <= p_len)
       corrected_source_into((float*)psrc_field.p, (const int*)psrc_idx.p, (const int*)psrc_slot.p, p_nsrc,
-                            (const float*)psrc_sig.p, p_nsig, (int)t, 0);
+                            (const float*)psrc_sig.p, p_nsig, (int)t, 0, (const float*)psrc_w.p);
     RhoArgs ra{};
     for (int a = 0; a < d.dim; ++a) {
       ra.S[a] = S[a + 1];
@@ -1041,6 +1188,7 @@ void Session::enqueue_step_body(uint64_t t) {
     ra.dsrc = pdense;
     ra.sens = sens_p;
     ra.clk = clk;
+    ra.S_rr = axisym ? (const float2*)S_buf[4].p : nullptr;
     if (eos == 1) {
       ra.p_loc = (float*)ploc_buf.p;
       ra.S_q = S[1];
@@ -1087,10 +1235,10 @@ void Session::enqueue_step_body(uint64_t t) {
 
 // corrected source field for "many" signals, using `work` as spectral scratch
 void Session::corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
-                                    int nrows_sig, int t, int work_i) {
+                                    int nrows_sig, int t, int work_i, const float* weight) {
   float2* work = (float2*)S_buf[work_i].p;
   ck(cudaMemsetAsync(out, 0, sizeof(float) * d.npts, st), "memset");
-  ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, st), "scatter");
+  ck(launch_scatter(out, idx, slot, n, sig, nrows_sig, t, weight, st), "scatter");
   ck(launch_x_r2c(out, work, d, plan[0], twd[0], rowL, st), "x_r2c");
   run_spectral({work_i}, {work_i}, {SpecOp{OP_SRC_KAPPA, 0}}, 1);
   ck(launch_x_c2r(work, out, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
@@ -1281,7 +1429,8 @@ void Session::read(kw_output* out) {
   if (p_rms_buf.p) ck(launch_rms_final((const float2*)p_rms_buf.p, (float*)p_rmsf_buf.p, ns, inv, st), "rms");
   for (int a = 0; a < d.dim; ++a)
     if (u_rms_buf[a].p) ck(launch_rms_final((const float2*)u_rms_buf[a].p, (float*)u_rmsf_buf[a].p, ns, inv, st), "rms");
-  const size_t ser = ring_rows ? 0 : (size_t)ns * (size_t)nrec, per = (size_t)ns, all = (size_t)d.npts;
+  const size_t ser = ring_rows ? 0 : (size_t)ns * (size_t)nrec, per = (size_t)ns;
+  const size_t all = axisym ? (size_t)d.nx * ny0 : (size_t)d.npts;  // axisymmetric: the unmirrored quarter
   d2h(out->p, p_raw_buf.p, ser, st);
   d2h(out->p_max, p_max_buf.p, per, st);
   d2h(out->p_min, p_min_buf.p, per, st);
@@ -1322,10 +1471,11 @@ Session::~Session() {
 }
 
 size_t Session::device_bytes_estimate(const kw_input* in, const kw_options* o) {
-  const size_t n = (size_t)(in->Nx * in->Ny * in->Nz);
+  const size_t n = (size_t)(in->Nx * in->Ny * in->Nz) * (in->axisymmetric_flag ? 4 : 1);
   const size_t dim = in->Nz == 1 ? 2 : 3;
   const size_t nxp = ((in->Nx / 2 + 1) + 1) / 2 * 2;
-  size_t b = 4 * 8 * nxp * in->Ny * in->Nz + 2 * dim * 4 * n;  // spectra, u, rho
+  const size_t nspec = in->axisymmetric_flag ? 5 : 4;
+  size_t b = nspec * 8 * nxp * (n / in->Nx) + 2 * dim * 4 * n;  // spectra, u, rho
   b += 4 * n * (2 + dim);                                       // medium maps
   return b;
 }

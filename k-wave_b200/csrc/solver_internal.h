@@ -64,9 +64,14 @@ class Session {
   void setup_sensors(const kw_input* in);
   void build_sensor_lists(const uint64_t* lin, size_t n, std::vector<int>& si, std::vector<int>& sl);
   void corrected_source(float* out, const int* idx, const int* slot, int n, const float* sig, int nrows_sig,
-                        int t);
+                        int t, const float* weight = nullptr);
   void corrected_source_into(float* out, const int* idx, const int* slot, int n, const float* sig,
-                             int nrows_sig, int t, int work_i);
+                             int nrows_sig, int t, int work_i, const float* weight = nullptr);
+  // axisymmetric inputs (Nx x Ny, y radial from the axis) become an ordinary
+  // 2D problem on Nx x 4Ny: the fields mirrored even about the axis and odd
+  // about the outer radius, as the reference's 'WSWA-FFT' symmetry mirrors
+  // them each step (kspaceFirstOrderAS.m:488-519, 709-722, 911-931)
+  const kw_input* expand_axisymmetric(const kw_input* in);
   void run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout);
   void col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs);
   void fused_pass(const std::vector<int>& ins, const std::vector<int>& outs, const std::vector<SpecOp>& ops,
@@ -110,10 +115,23 @@ class Session {
   DevBuf c0sq_buf, rho0_buf, rinv_buf[3], bona_buf, c2tau_buf, c2eta_buf;
   Map c0sq_m{}, rho0_m{}, rinv_m[3]{}, bona_m{}, c2tau_m{}, c2eta_m{}, tau_m{};
   // fields
-  DevBuf u_buf[3], rho_buf[3], S_buf[4], ploc_buf, p_buf, p0_buf, clock_buf, err_buf;
+  DevBuf u_buf[3], rho_buf[3], S_buf[5], ploc_buf, p_buf, p0_buf, clock_buf, err_buf;
+  // axisymmetric state: the original radial size, the expanded inputs, the
+  // mirrored pressure-source entries (original entry, sign) and 1 / r
+  bool axisym = false;
+  int ny0 = 0;
+  struct AxisymmetricInput {
+    kw_input in;
+    std::vector<float> c0, rho0, sgx, sgy, bona, alpha, p0;
+    std::vector<uint64_t> p_idx;
+    std::vector<int> p_orig;
+    std::vector<float> p_w;
+  } asx;
+  uint64_t p_rows0 = 0;  // pressure-source points before mirroring
+  DevBuf psrc_w, inv_r_buf, ur_buf;
   // TMA tensor maps over the half-spectrum buffers (y pass / z pass)
   bool use_tma[3]{false, false, false};
-  CUtensorMap map_y[4], map_z[4];
+  CUtensorMap map_y[5], map_z[5];  // [4]: the axisymmetric u_r / r spectrum
   Clock clk{};
   // sources
   SparseSource psrc{}, usrc{};

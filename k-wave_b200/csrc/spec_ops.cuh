@@ -82,6 +82,12 @@ __device__ __forceinline__ float2 eval_op(const SpecOp& op, const SpecTables& T,
       const float2 d = __ldg(T.shift_neg[op.axis] + id);
       return make_float2(d.x * T.scale, d.y * T.scale);
     }
+    case OP_KAPPA_SHIFT_NEG: {
+      const int id = op.axis == 0 ? ix : (op.axis == 1 ? iy : iz);
+      const float2 d = __ldg(T.shift_neg[op.axis] + id);
+      const float s = sinc_series(T.cdt2 * k) * T.scale;
+      return make_float2(d.x * s, d.y * s);
+    }
     case OP_SRC_KAPPA:
       return make_float2(cos_series(T.cdt2 * k) * T.scale, 0.f);
     default:

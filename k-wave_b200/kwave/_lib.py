@@ -60,6 +60,7 @@ class KwInput(C.Structure):
         ("transducer_source_flag", C.c_uint64), ("transducer_source_input", c_float_p),
         ("transducer_source_input_numel", C.c_uint64), ("delay_mask", c_u64_p),
         ("transducer_source_apodization", c_float_p),
+        ("axisymmetric_flag", C.c_uint64),
     ]
 
 
@@ -249,6 +250,7 @@ def make_input(inp: dict):
             sig = np.asarray(inp[f"u{a}_source_input"], dtype=np.float32)
             sig = sig.reshape(-1, sig.shape[-1]) if sig.ndim > 1 else sig.reshape(1, -1)
             setattr(s, f"u{a}_source_input", _fptr(keep.f32(sig)))
+    s.axisymmetric_flag = int(inp.get("axisymmetric_flag", 0))
     s.transducer_source_flag = int(inp.get("transducer_source_flag", 0))
     if u_any or s.transducer_source_flag:
         s.u_source_mode = int(inp.get("u_source_mode", 0))

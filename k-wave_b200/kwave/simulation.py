@@ -119,7 +119,8 @@ def _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0):
 
 
 def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_size=None,
-            pml_alpha=None, pml_inside=True, smooth_p0=True, data_cast="single", cart_interp="nearest"):
+            pml_alpha=None, pml_inside=True, smooth_p0=True, data_cast="single", cart_interp="nearest",
+            axisymmetric=False):
     """Build the datasets of the HDF5 input file (saveToDisk.m:44-378)
     plus the record list / start index the wrapper turns into flags.
 
@@ -129,9 +130,22 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
     vertices around each point and interpolates the series in postprocess()
     (the in-memory solvers' default, kspaceFirstOrder_extractSensorData.m:296-420).
 
+    ``axisymmetric`` is kspaceFirstOrderAS: a 2D grid with x axial and y
+    radial (the axis on the first row of y); absorption is Stokes
+    (kspaceFirstOrder_inputChecking.m:172-199).
+
     Returns (inp, record, start_index, meta)."""
     if cart_interp not in ("nearest", "linear"):
         raise ValueError("cart_interp must be 'nearest' or 'linear'")
+    if axisymmetric:
+        if kgrid.dim != 2:
+            raise ValueError("axisymmetric simulations need a 2D grid")
+        if not pml_inside:
+            raise NotImplementedError("PMLInside = false is not supported for axisymmetric simulations")
+        if isinstance(source, KWaveTransducer) or isinstance(sensor, KWaveTransducer):
+            raise ValueError("Transducer inputs are only compatible with 3D simulations.")
+        if any(k in source for k in ("ux", "uy", "u_mask")):
+            raise NotImplementedError("velocity sources are not supported for axisymmetric simulations")
     dim = kgrid.dim
     if kgrid.dt is None or kgrid.Nt is None:
         kgrid.make_time(medium["sound_speed"])
@@ -185,7 +199,7 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         inp["nonlinear_flag"] = 1
         inp["BonA"] = _as_grid(medium["BonA"], shape)
     if "alpha_coeff" in medium:
-        stokes = medium.get("alpha_mode") == "stokes"
+        stokes = medium.get("alpha_mode") == "stokes" or axisymmetric
         y = 2.0 if stokes else float(medium["alpha_power"])
         if not stokes and y == 1.0:
             raise ValueError("medium.alpha_power = 1 is not supported (the dispersion term is singular)")
@@ -198,7 +212,10 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         p0 = np.asarray(source["p0"], dtype=np.float64)
         if p0.shape != tuple(shape):
             raise ValueError("source.p0 must be the same size as the computational grid.")
-        if smooth_p0:
+        if smooth_p0 and axisymmetric:
+            # smoothed on the mirrored grid (kspaceFirstOrder_inputChecking.m:1504-1533)
+            p0 = smooth(_mirror_wswa(p0), True)[:, :shape[1]]
+        elif smooth_p0:
             p0 = smooth(p0, True)
         inp["p0_source_flag"] = 1
         inp["p0_source_input"] = p0
@@ -306,10 +323,30 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
             raw.append("u_non_staggered")
         meta["interp"]["record"] = list(record)
         record = grid_out + raw
+    if axisymmetric:
+        if meta.get("reorder_index") is not None or meta.get("interp") is not None:
+            raise NotImplementedError("Cartesian sensor masks are not supported for axisymmetric simulations")
+        if any(r in record for r in ("u_non_staggered", "I", "I_avg")):
+            raise NotImplementedError("u_non_staggered and intensity are not supported for axisymmetric simulations")
+        inp["axisymmetric_flag"] = 1
     start = int(sensor.get("record_start_index", 1))
     meta["user_record"] = list(sensor.get("record", ["p"]))
     meta["has_record"] = "record" in sensor
     return inp, record, start, meta
+
+
+def _mirror_wswa(a):
+    """The 'WSWA-FFT' radial mirror of a field on the pressure points:
+    columns [a, 0, -flip(a[:, 1:]), -a, 0, flip(a[:, 1:])]
+    (kspaceFirstOrderAS.m:711-714)."""
+    a = np.asarray(a, dtype=np.float64)
+    ny = a.shape[1]
+    out = np.zeros((a.shape[0], 4 * ny))
+    out[:, :ny] = a
+    out[:, ny + 1:2 * ny] = -a[:, 1:][:, ::-1]
+    out[:, 2 * ny:3 * ny] = -a
+    out[:, 3 * ny + 1:] = a[:, 1:][:, ::-1]
+    return out
 
 
 def fourier_shift(data, shift, axis=-1):
@@ -418,3 +455,8 @@ def kspace_first_order(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dic
 
 kspaceFirstOrder2D = kspace_first_order
 kspaceFirstOrder3D = kspace_first_order
+
+
+def kspaceFirstOrderAS(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, device=-1, **options):
+    """The axisymmetric solver (kspaceFirstOrderAS.m): x axial, y radial."""
+    return kspace_first_order(kgrid, medium, source, sensor, device=device, axisymmetric=True, **options)

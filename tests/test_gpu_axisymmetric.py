@@ -1,0 +1,109 @@
+"""Axisymmetric solver on the GPU (kspaceFirstOrderAS.m) against the
+axisymmetric oracle, on the TMA and non-TMA radial sizes, through kw_solve,
+the input file and the front end."""
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_LOSSLESS = 1e-5
+TOL = 1e-4
+
+
+def _inputs(nx, ny, nt, het=False, seed=3):
+    rng = np.random.default_rng(seed)
+    dx = 1e-4
+    c = 1500 + 40 * rng.random((nx, ny)) if het else 1500.0
+    rho = 1000 + 30 * rng.random((nx, ny)) if het else 1000.0
+    c_ref = float(np.max(c))
+    xx = np.arange(nx)[:, None] - nx // 2
+    yy = np.arange(ny)[None, :]
+    p0 = 2 * np.exp(-(xx.astype(float) ** 2 + (yy - 3.0) ** 2) / 5.0)
+    mask = np.zeros((nx, ny))
+    mask[::3, ::2] = 1
+    return dict(Nx=nx, Ny=ny, Nz=1, Nt=nt, dx=dx, dy=dx, dz=0.0, dt=0.3 * dx / c_ref, c_ref=c_ref, c0=c,
+                rho0=rho, rho0_sgx=rho, rho0_sgy=rho, pml_x_size=6, pml_y_size=6, pml_z_size=0,
+                pml_x_alpha=2.0, pml_y_alpha=2.0, pml_z_alpha=0.0, p0_source_flag=1, p0_source_input=p0,
+                sensor_mask_type=0, sensor_mask_index=np.flatnonzero(mask.reshape(-1, order="F")) + 1,
+                axisymmetric_flag=1)
+
+
+def _check(inp, record, tol, start=1):
+    from kwave import _lib
+    from oracle.kspace_oracle_as import simulate_as
+
+    gpu = _lib.solve(inp, record=record, start_index=start)
+    ora = simulate_as(inp, record=record, record_start_index=start, dtype=np.float64)
+    errs = {k: rel_l2(gpu[k], ora[k]) for k in ora if k in gpu}
+    assert errs and max(errs.values()) <= tol, errs
+    for k in ("p_final", "ux_final", "p_max_all"):
+        if k in gpu:
+            assert gpu[k].shape == (inp["Nx"], inp["Ny"]), k
+    return gpu
+
+
+@pytest.mark.parametrize("ny", [64, 20])  # expanded radial lengths 256 (TMA) and 80
+def test_p0_lossless(ny):
+    inp = _inputs(48, ny, 60)
+    _check(inp, ("p", "p_max", "p_rms", "u", "u_max", "p_final", "u_final", "p_max_all", "p_min_all"),
+           TOL_LOSSLESS)
+
+
+def test_het_nonlinear_stokes_sources():
+    base = _inputs(64, 32, 70, het=True)
+    base.update(p0_source_flag=0, nonlinear_flag=1, BonA=5.0, absorbing_flag=2, alpha_coeff=0.75)
+    t = np.arange(40) * base["dt"]
+    sig = 1e3 * np.sin(2 * np.pi * 2e6 * t) * np.hanning(40)
+    idx = np.array([20 + 64 * 0, 20 + 64 * 4, 33 + 64 * 9]) + 1  # on the axis and off it
+    rec = ("p", "p_max", "p_min", "u", "p_final")
+    for mode, many in ((2, 0), (1, 1), (0, 0), (2, 1)):
+        inp = dict(base)
+        s = sig[None, :] * (1 + 0.2 * np.arange(3)[:, None]) if many else sig[None, :]
+        # scaled density increments (kspaceFirstOrder_scaleSourceTerms.m): about 1e-3 kg/m^3
+        inp.update(p_source_flag=40, p_source_mode=mode, p_source_many=many, p_source_index=idx,
+                   p_source_input=1e-6 * s)
+        _check(inp, rec, TOL, start=5)
+
+
+def test_input_file_matches_solve(tmp_path):
+    from kwave import _lib, h5io
+
+    inp = _inputs(48, 32, 40, het=True)
+    rec = ("p", "p_final", "u_max")
+    fin, fout = tmp_path / "as_in.h5", tmp_path / "as_out.h5"
+    h5io.write_input_file(fin, inp)
+    _lib.run_file(fin, fout, rec)
+    got = h5io.read_output_file(fout, 2)
+    want = _lib.solve(inp, record=rec)
+    for k in want:
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
+def test_front_end():
+    from kwave import kspaceFirstOrderAS
+    from kwave.simulation import postprocess, prepare
+    from kwave.utils import KWaveGrid, make_disc
+    from oracle.kspace_oracle_as import simulate_as
+
+    kg = KWaveGrid((64, 32), (1e-4, 1e-4))
+    kg.set_time(50, 0.3e-4 / 1500)
+    p0 = 3 * make_disc(64, 32, 32, 1, 5)
+    sensor = {"mask": np.pad(np.ones((1, 10)), ((40, 23), (0, 22))), "record": ["p", "p_max"]}
+    medium = {"sound_speed": 1500.0, "density": 1000.0}
+    out = kspaceFirstOrderAS(kg, medium, {"p0": p0}, sensor, pml_size=8)
+    inp, record, start, meta = prepare(kg, medium, {"p0": p0}, sensor, pml_size=8, axisymmetric=True)
+    ora = postprocess(simulate_as(inp, record=record, dtype=np.float64), inp, meta)
+    assert rel_l2(out["p"], ora["p"]) <= TOL_LOSSLESS and rel_l2(out["p_max"], ora["p_max"]) <= TOL_LOSSLESS
+
+
+def test_rejects_what_it_does_not_run():
+    from kwave import _lib
+
+    inp = _inputs(32, 16, 10)
+    bad = dict(inp, absorbing_flag=1, alpha_coeff=0.5, alpha_power=1.5)
+    with pytest.raises(_lib.KwaveError, match="Stokes"):
+        _lib.solve(bad, record=("p",))
+    with pytest.raises(_lib.KwaveError, match="u_non_staggered"):
+        _lib.solve(inp, record=("u_non_staggered",))
