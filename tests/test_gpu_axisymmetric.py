@@ -107,3 +107,33 @@ def test_rejects_what_it_does_not_run():
         _lib.solve(bad, record=("p",))
     with pytest.raises(_lib.KwaveError, match="u_non_staggered"):
         _lib.solve(inp, record=("u_non_staggered",))
+
+
+def test_tester_axisymmetric_case():
+    """The reference harness's axisymmetric configuration (kWaveTester.m
+    test_dim 4, grid type 1): 128 x 64, PML 20 / 10 inside, heterogeneity x1.3
+    in the far half of a disc of radius 10, Stokes absorption with y = 2,
+    B/A 6, an initial-pressure disc of radius 5, CFL 0.1."""
+    from kwave import _lib
+    from kwave.simulation import postprocess, prepare
+    from kwave.utils import KWaveGrid, make_disc
+    from oracle.kspace_oracle_as import simulate_as
+
+    nx, ny = 128, 64
+    dx = 40e-3 / nx
+    kg = KWaveGrid((nx, ny), (dx, dx))
+    het = make_disc(nx, 2 * ny, nx // 2, ny // 2, 10)[:, ny:] == 1
+    medium = {"sound_speed": np.where(het, 1540 * 1.3, 1540.0), "density": np.where(het, 1300.0, 1000.0),
+              "BonA": np.where(het, 7.8, 6.0), "alpha_coeff": np.where(het, 0.975, 0.75), "alpha_power": 2.0,
+              "alpha_mode": "stokes"}
+    kg.make_time(medium["sound_speed"], cfl=0.1)
+    kg.set_time(120, kg.dt)
+    mask = np.zeros((nx, ny))
+    mask[::4, ::3] = 1
+    sensor = {"mask": mask, "record": ["p", "p_max", "u", "p_final"]}
+    src = {"p0": 1e6 * make_disc(nx, ny, nx // 2, ny // 2, 5)}
+    inp, record, start, meta = prepare(kg, medium, src, sensor, pml_size=(20, 10), axisymmetric=True)
+    gpu = postprocess(_lib.solve(inp, record=record, start_index=start), inp, meta)
+    ora = postprocess(simulate_as(inp, record=record, record_start_index=start, dtype=np.float64), inp, meta)
+    errs = {k: rel_l2(gpu[k], ora[k]) for k in ora}
+    assert max(errs.values()) <= TOL, errs
