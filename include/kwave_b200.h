@@ -137,6 +137,20 @@ typedef struct {
    * Stokes media (absorbing_flag 0 or 2), with or without B/A.
    */
   uint64_t axisymmetric_flag;
+
+  /*
+   * Cartesian sensor points by linear interpolation (the in-memory solvers'
+   * 'CartInterp' 'linear', kspaceFirstOrder_extractSensorData.m:296-420):
+   * for each point, Nd + 1 vertex indices (1-based linear) and barycentric
+   * weights, point-major (point j uses entries j*(Nd+1) .. j*(Nd+1)+Nd).
+   * When set, sensor_mask_type must be 0, sensor_mask_index is not read,
+   * and the sensor outputs are per point, interpolated on the device every
+   * step; the full-grid outputs are unaffected.  No input-file dataset
+   * carries this.
+   */
+  const uint64_t* sensor_interp_index;
+  const float* sensor_interp_weight;
+  uint64_t sensor_interp_numel; /* points * (Nd + 1) */
 } kw_input;
 
 /* What to record, and run settings: the binary's command-line flags. */

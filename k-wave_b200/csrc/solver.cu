@@ -52,6 +52,8 @@ cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Ma
                             long long n, cudaStream_t st);
 cudaError_t launch_scale_rows(float* out, const float* in, const float* r, int nx, int ny, long long n,
                               cudaStream_t st);
+cudaError_t launch_interp_sensor(const Sensor& s, const float* vals, const int* vslot, const float* w, int K,
+                                 const Clock& clk, cudaStream_t st);
 cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& clk, long long n,
                                 cudaStream_t st);
 cudaError_t launch_advance(int* t, cudaStream_t st);
@@ -876,7 +878,27 @@ Dims Session::slab_dims(int z0, int nzs) const {
 
 void Session::setup_sensors(const kw_input* in) {
   std::vector<int> si, sl;
-  if (in->sensor_mask_type == 0) {
+  std::vector<int> vslot;
+  if (in->sensor_interp_index) {
+    // Cartesian points by linear interpolation: record the distinct
+    // vertices, form the points on the device
+    interp_k = d.dim + 1;
+    if (!in->sensor_interp_weight || in->sensor_interp_numel == 0 || in->sensor_interp_numel % interp_k)
+      throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_interp_index / _weight must hold Nd + 1 entries per point");
+    if (in->sensor_mask_type != 0) throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor interpolation needs sensor_mask_type 0");
+    std::vector<uint64_t> verts(in->sensor_interp_index, in->sensor_interp_index + in->sensor_interp_numel);
+    for (uint64_t v : verts)
+      if (v < 1 || v > (uint64_t)d.npts) throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_interp_index holds an index outside the grid");
+    std::sort(verts.begin(), verts.end());
+    verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
+    vslot.resize(in->sensor_interp_numel);
+    for (uint64_t e = 0; e < in->sensor_interp_numel; ++e)
+      vslot[e] = (int)(std::lower_bound(verts.begin(), verts.end(), in->sensor_interp_index[e]) - verts.begin());
+    nvert = (long long)verts.size();
+    build_sensor_lists(verts.data(), verts.size(), si, sl);
+    interp = true;
+    ns = (long long)(in->sensor_interp_numel / interp_k);
+  } else if (in->sensor_mask_type == 0) {
     if (!in->sensor_mask_index || in->sensor_mask_index_numel == 0)
       throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_mask_index missing");
     ns = (long long)in->sensor_mask_index_numel;
@@ -927,12 +949,29 @@ void Session::setup_sensors(const kw_input* in) {
   // sensor state for p and u
   auto mk = [&](Sensor& s) {
     s = Sensor{};
-    s.mode = dense_sensor ? 1 : 2;
+    s.mode = interp ? 3 : (dense_sensor ? 1 : 2);
     s.ns = (int)ns;
     s.ring = (int)ring_rows;
+    s.idx = (dense_sensor || interp) ? nullptr : sidx_d;
+    s.slot = (dense_sensor || interp) ? nullptr : sslot_d;
+  };
+  // the vertices' values of this step (one row, always overwritten)
+  auto mkv = [&](Sensor& s, DevBuf& vals) {
+    s = Sensor{};
+    s.mode = dense_sensor ? 1 : 2;
+    s.ns = (int)nvert;
+    s.ring = 1;
     s.idx = dense_sensor ? nullptr : sidx_d;
     s.slot = dense_sensor ? nullptr : sslot_d;
+    vals.alloc(sizeof(float) * (size_t)nvert, st);
+    ck(cudaMemsetAsync(vals.p, 0, sizeof(float) * (size_t)nvert, st), "memset");
+    s.raw = (float*)vals.p;
   };
+  if (interp) {
+    up(vslot_buf, vslot.data(), vslot.size(), st);
+    std::vector<float> w(in->sensor_interp_weight, in->sensor_interp_weight + in->sensor_interp_numel);
+    up(vweight_buf, w.data(), w.size(), st);
+  }
   mk(sens_p);
   const size_t ser = sizeof(float) * (size_t)ns * (size_t)(ring_rows ? ring_rows : nrec);
   if (ring_rows && sens_p.ring != ring_rows)
@@ -979,6 +1018,46 @@ void Session::setup_sensors(const kw_input* in) {
     }
     uns_field_buf.alloc(all, st);
   }
+  if (interp) {
+    // the step kernels see the vertex sensors; the full-grid reductions,
+    // which do not depend on the mask, move there with them
+    auto split = [&](Sensor& pt, Sensor& vs, DevBuf& vals) {
+      const bool per_point = pt.raw || pt.vmax || pt.vmin || pt.rms;
+      if (!per_point && !pt.max_all && !pt.min_all) {
+        vs = Sensor{};
+        return;
+      }
+      mkv(vs, vals);
+      if (!per_point) vs.raw = nullptr;
+      vs.max_all = pt.max_all;
+      vs.min_all = pt.min_all;
+      pt.max_all = pt.min_all = nullptr;
+      if (!per_point) pt.mode = 0;
+    };
+    split(sens_p, vsens_p, vval_p_buf);
+    for (int a = 0; a < d.dim; ++a) {
+      split(sens_u[a], vsens_u[a], vval_u_buf[a]);
+      if (sens_uns[a].mode) split(sens_uns[a], vsens_uns[a], vval_uns_buf[a]);
+    }
+  }
+}
+
+void Session::interp_points(int which) {
+  if (!interp) return;
+  const int* vs = (const int*)vslot_buf.p;
+  const float* w = (const float*)vweight_buf.p;
+  if (which == 0 && vsens_p.raw) {
+    ck(launch_interp_sensor(sens_p, vsens_p.raw, vs, w, interp_k, clk, st), "interp p");
+    ++launches_;
+  }
+  for (int a = 0; a < d.dim; ++a) {
+    const Sensor& pt = (which == 1) ? sens_u[a] : sens_uns[a];
+    const Sensor& vx = (which == 1) ? vsens_u[a] : vsens_uns[a];
+    if (which != 0 && vx.raw) {
+      ck(launch_interp_sensor(pt, vx.raw, vs, w, interp_k, clk, st), "interp u");
+      ++launches_;
+    }
+  }
 }
 
 // u on the regular grid at the sensors (kspaceFirstOrder_extractSensorData.m:109-120):
@@ -993,9 +1072,10 @@ void Session::record_non_staggered() {
     ck(launch_x_r2c((const float*)u_buf[a].p, work, d, plan[0], twd[0], rowL, st), "x_r2c");
     run_spectral({0}, {0}, {SpecOp{OP_SHIFT_NEG, a}}, 1);
     ck(launch_x_c2r(work, f, 0, d, plan[0], twd[0], rowL, st), "x_c2r");
-    ck(launch_record_field(f, sens_uns[a], clk, d.npts, st), "record");
+    ck(launch_record_field(f, row_sens_uns(a), clk, d.npts, st), "record");
     launches_ += 3;  // r2c, c2r, record (the spectral passes count themselves)
   }
+  interp_points(2);
 }
 
 void Session::build_sensor_lists(const uint64_t* lin, size_t n, std::vector<int>& si, std::vector<int>& sl) {
@@ -1029,7 +1109,8 @@ void Session::build_sensor_lists(const uint64_t* lin, size_t n, std::vector<int>
 // p = p0, rho_i = p0 / (dim c0^2), u_i = dt rho0_sg_inv grad_i(p0) / 2.
 void Session::enqueue_init() {
   const float* p0d = (const float*)p0_buf.p;
-  ck(launch_record_field(p0d, sens_p, clk, d.npts, st), "record p0");
+  ck(launch_record_field(p0d, row_sens_p(), clk, d.npts, st), "record p0");
+  interp_points(0);
   ++launches_;
   ck(launch_rho_init((float*)rho_buf[0].p, (float*)rho_buf[1].p, d.dim == 3 ? (float*)rho_buf[2].p : nullptr,
                      p0d, c0sq_m, d.dim, d.npts, st), "rho init");
@@ -1046,6 +1127,7 @@ void Session::enqueue_init() {
   ua.init = 1;
   ua.do_r2c = 0;
   ck(launch_x_u(ua, d, plan[0], twd[0], rowL, st), "x_u init");
+  interp_points(1);
   ++launches_;
   record_non_staggered();
   // the x and y transforms of p for the next step's gradient
@@ -1068,7 +1150,7 @@ UArgs Session::u_args(float2* const* S) {
     ua.src_sig[a] = usig_d[a];
     ua.src_len[a] = u_len[a];
     ua.dsrc[a] = udense[a];
-    ua.sens[a] = sens_u[a];
+    ua.sens[a] = row_sens_u(a);
   }
   ua.dt = dtf;
   ua.init = 0;
@@ -1154,6 +1236,7 @@ void Session::enqueue_step_body(uint64_t t) {
       ck(launch_x_r2c((const float*)ur_buf.p, (float2*)S_buf[4].p, d, plan[0], twd[0], rowL, st), "x_r2c");
       launches_ += 2;
     }
+    interp_points(1);
     record_non_staggered();
     // (2) mass conservation: div u -> rho, EOS (:905-1017)
     {
@@ -1186,7 +1269,7 @@ void Session::enqueue_step_body(uint64_t t) {
     ra.tau = tau_m;
     ra.src = psrc;
     ra.dsrc = pdense;
-    ra.sens = sens_p;
+    ra.sens = row_sens_p();
     ra.clk = clk;
     ra.S_rr = axisym ? (const float2*)S_buf[4].p : nullptr;
     if (eos == 1) {
@@ -1207,6 +1290,7 @@ void Session::enqueue_step_body(uint64_t t) {
       else
         col_pass(false, {0}, z0, nzs);
     }
+    if (eos != 1) interp_points(0);
     if (eos == 1) {
       // (3) power-law absorption and dispersion (:970-977)
       fused_pass(f12, f12, {SpecOp{OP_NABLA1, 0}, SpecOp{OP_NABLA2, 0}}, 1);
@@ -1218,7 +1302,7 @@ void Session::enqueue_step_body(uint64_t t) {
       ea.c2eta = c2eta_m;
       ea.p_out = last ? (float*)p_buf.p : nullptr;
       ea.S_p = S[0];
-      ea.sens = sens_p;
+      ea.sens = row_sens_p();
       ea.clk = clk;
       for (int z0 = 0; z0 < d.nz; z0 += slab) {
         const int nzs = std::min(slab, d.nz - z0);
@@ -1227,6 +1311,7 @@ void Session::enqueue_step_body(uint64_t t) {
         ++launches_;
         col_pass(false, {0}, z0, nzs);
       }
+      interp_points(0);
     }
   }
   ck(launch_advance((int*)clock_buf.p, st), "advance");
@@ -1531,7 +1616,11 @@ int kw_output_sizes_query(const kw_input* in, const kw_options* opt, kw_output_s
     if (in->Nx < 1 || in->Ny < 1 || in->Nz < 1 || in->Nt < 1)
       throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
     uint64_t nsens = 0;
-    if (in->sensor_mask_type == 0) {
+    if (in->sensor_interp_index) {
+      const uint64_t k = (in->Nz == 1 ? 3 : 4);
+      if (in->sensor_interp_numel % k) throw KwError(KW_ERR_INVALID_ARGUMENT, "sensor_interp_numel must be a multiple of Nd + 1");
+      nsens = in->sensor_interp_numel / k;
+    } else if (in->sensor_mask_type == 0) {
       nsens = in->sensor_mask_index_numel;
     } else if (in->sensor_mask_type == 1) {
       if (!in->sensor_mask_corners || in->sensor_mask_corners_numel % 6)

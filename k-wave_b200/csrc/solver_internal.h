@@ -153,6 +153,18 @@ class Session {
   const int* sslot_d = nullptr;
   Sensor sens_p{}, sens_u[3]{};
   Sensor sens_uns[3]{};                 // u on the regular grid (u_non_staggered_raw)
+  // Cartesian points by linear interpolation: the step kernels record the
+  // simplex vertices (vsens_*, this step only), k_interp_sensor forms the
+  // points (sens_*, mode 3) from them
+  bool interp = false;
+  int interp_k = 0;
+  long long nvert = 0;
+  Sensor vsens_p{}, vsens_u[3]{}, vsens_uns[3]{};
+  DevBuf vslot_buf, vweight_buf, vval_p_buf, vval_u_buf[3], vval_uns_buf[3];
+  const Sensor& row_sens_p() const { return interp ? vsens_p : sens_p; }
+  const Sensor& row_sens_u(int a) const { return interp ? vsens_u[a] : sens_u[a]; }
+  const Sensor& row_sens_uns(int a) const { return interp ? vsens_uns[a] : sens_uns[a]; }
+  void interp_points(int which);  // 0: p, 1: u, 2: u on the regular grid
   DevBuf uns_raw_buf[3], uns_field_buf;  // its series; the shifted field of one component
   void record_non_staggered();
   DevBuf p_raw_buf, p_max_buf, p_min_buf, p_rms_buf, p_rmsf_buf, p_maxall_buf, p_minall_buf;

@@ -61,6 +61,8 @@ class KwInput(C.Structure):
         ("transducer_source_input_numel", C.c_uint64), ("delay_mask", c_u64_p),
         ("transducer_source_apodization", c_float_p),
         ("axisymmetric_flag", C.c_uint64),
+        ("sensor_interp_index", c_u64_p), ("sensor_interp_weight", c_float_p),
+        ("sensor_interp_numel", C.c_uint64),
     ]
 
 
@@ -266,7 +268,17 @@ def make_input(inp: dict):
         if inp.get("transducer_source_apodization") is not None:
             s.transducer_source_apodization = _fptr(keep.f32(inp["transducer_source_apodization"]))
     s.sensor_mask_type = int(inp.get("sensor_mask_type", 0))
-    if s.sensor_mask_type == 0:
+    if inp.get("sensor_interp_index") is not None:
+        # (points, Nd + 1) arrays, flattened point-major (C order)
+        vi = np.ascontiguousarray(np.asarray(inp["sensor_interp_index"], dtype=np.uint64).reshape(-1))
+        vw = np.ascontiguousarray(np.asarray(inp["sensor_interp_weight"], dtype=np.float32).reshape(-1))
+        keep.arrays += [vi, vw]
+        if vi.size != vw.size:
+            raise ValueError("sensor_interp_index and sensor_interp_weight differ in size")
+        s.sensor_interp_index = _uptr(vi)
+        s.sensor_interp_weight = _fptr(vw)
+        s.sensor_interp_numel = vi.size
+    elif s.sensor_mask_type == 0:
         idx = keep.u64(inp["sensor_mask_index"])
         s.sensor_mask_index = _uptr(idx)
         s.sensor_mask_index_numel = idx.size

@@ -213,6 +213,8 @@ def write_input_file(path, inp: dict, description="input written by kwave.h5io")
     A transducer's transmit apodization has no dataset in the format (the
     reference's writer, kspaceFirstOrder_saveToDisk.m:289-293, 339-343,
     drops it too); it is left out with a warning unless it is all ones."""
+    if inp.get("sensor_interp_index") is not None:
+        raise ValueError("the input file format has no interpolated Cartesian sensors: use cart_interp='nearest'")
     apod = inp.get("transducer_source_apodization")
     if apod is not None and np.any(np.asarray(apod) != 1):
         warnings.warn("the input file format has no transmit apodization: it is dropped", stacklevel=2)

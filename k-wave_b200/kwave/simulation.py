@@ -126,9 +126,11 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
 
     ``cart_interp`` is the reference's 'CartInterp' for Cartesian sensor
     points: "nearest" maps them to grid points, the only form an input file
-    can hold (kspaceFirstOrder_saveToDisk.m:35-37); "linear" records the
-    vertices around each point and interpolates the series in postprocess()
-    (the in-memory solvers' default, kspaceFirstOrder_extractSensorData.m:296-420).
+    can hold (kspaceFirstOrder_saveToDisk.m:35-37); "linear" passes each
+    point's simplex vertices and barycentric weights
+    (``sensor_interp_index`` / ``sensor_interp_weight``) and the solver
+    interpolates every step (the in-memory solvers' default,
+    kspaceFirstOrder_extractSensorData.m:296-420).
 
     ``axisymmetric`` is kspaceFirstOrderAS: a 2D grid with x axial and y
     radial (the axis on the first row of y); absorption is Stokes
@@ -290,13 +292,14 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         meta["cuboid"] = True
         meta["corners"] = corners
     elif mask.ndim == 2 and mask.shape[0] == dim and cart_interp == "linear":
-        # Cartesian points, linear interpolation: record the vertices of the
-        # simplices holding the points, interpolate on the host
+        # Cartesian points, linear interpolation: the solver records the
+        # vertices of the simplex around each point and forms the point
+        # every step (kspaceFirstOrder_extractSensorData.m:296-420)
         verts, w = cart_linear_weights(kgrid, mask)
-        uniq = np.unique(verts)
         inp["sensor_mask_type"] = 0
-        inp["sensor_mask_index"] = uniq
-        meta["interp"] = {"col": np.searchsorted(uniq, verts), "w": w}
+        inp["sensor_interp_index"] = verts
+        inp["sensor_interp_weight"] = w
+        meta["interp"] = True
     elif mask.ndim == 2 and mask.shape[0] == dim:
         # Cartesian points: nearest-neighbour mapping, as the file path requires
         # (kspaceFirstOrder_saveToDisk.m:35-37; createStorageVariables.m:33-51)
@@ -310,21 +313,8 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
         record = [r for r in record if r not in ("I", "I_avg")] + [r for r in ("u_non_staggered", "p")
                                                                    if r not in record]
         meta["intensity"] = [r for r in sensor["record"] if r in ("I", "I_avg")]
-    if meta.get("interp") is not None:
-        # the simplex vertices record whole series; per-point reductions are
-        # taken on the interpolated series (kspaceFirstOrder_extractSensorData.m)
-        grid_out = [r for r in record if r.endswith("_all") or r.endswith("_final")]
-        raw = []
-        if any(r in record for r in ("p", "p_max", "p_min", "p_rms")):
-            raw.append("p")
-        if any(r in record for r in ("u", "u_max", "u_min", "u_rms")):
-            raw.append("u")
-        if "u_non_staggered" in record:
-            raw.append("u_non_staggered")
-        meta["interp"]["record"] = list(record)
-        record = grid_out + raw
     if axisymmetric:
-        if meta.get("reorder_index") is not None or meta.get("interp") is not None:
+        if meta.get("reorder_index") is not None or meta.get("interp"):
             raise NotImplementedError("Cartesian sensor masks are not supported for axisymmetric simulations")
         if any(r in record for r in ("u_non_staggered", "I", "I_avg")):
             raise NotImplementedError("u_non_staggered and intensity are not supported for axisymmetric simulations")
@@ -364,32 +354,6 @@ def fourier_shift(data, shift, axis=-1):
     return np.real(sfft.ifft(op * sfft.fft(data, axis=axis), axis=axis))
 
 
-def _interpolate_sensors(out, meta, dim):
-    """Cartesian sensors with linear interpolation: weighted sums of the
-    vertex series, then the requested per-point reductions of the
-    interpolated series."""
-    col, w, rec = meta["interp"]["col"], meta["interp"]["w"], meta["interp"]["record"]
-    series = ["p"] + [f"u{c}" for c in "xyz"[:dim]] + [f"u{c}_non_staggered" for c in "xyz"[:dim]]
-    for k in series:
-        if k in out:
-            v = np.asarray(out[k], dtype=np.float64)
-            out[k] = np.einsum("pj,pjt->pt", w, v[col]).astype(np.float32)
-    comps = {"p": ["p"], "u": [f"u{c}" for c in "xyz"[:dim]]}
-    for base, keys in comps.items():
-        for k in keys:
-            if k not in out:
-                continue
-            v = out[k].astype(np.float64)
-            if f"{base}_max" in rec:
-                out[f"{k}_max"] = v.max(axis=1).astype(np.float32)
-            if f"{base}_min" in rec:
-                out[f"{k}_min"] = v.min(axis=1).astype(np.float32)
-            if f"{base}_rms" in rec:
-                out[f"{k}_rms"] = np.sqrt(np.mean(v * v, axis=1)).astype(np.float32)
-            if base not in rec and not (base == "p" and meta.get("intensity")):
-                out.pop(k)
-
-
 def postprocess(out: dict, inp: dict, meta: dict):
     """Intensity, Cartesian reorder and cuboid reshape
     (kspaceFirstOrder_saveIntensity.m:42-75, _reorderCartData.m,
@@ -399,8 +363,6 @@ def postprocess(out: dict, inp: dict, meta: dict):
         for k in list(out):
             if k.endswith("_all") or k.endswith("_final"):
                 out[k] = out[k][meta["trim"]]
-    if meta.get("interp") is not None:
-        _interpolate_sensors(out, meta, dim)
     if meta.get("intensity"):
         for c in "xyz"[:dim]:
             u_sgt = fourier_shift(out[f"u{c}_non_staggered"], 0.5, axis=-1)

@@ -272,10 +272,24 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
     # sensor
     mask_type = int(inp.get("sensor_mask_type", 0))
     if mask_type == 0:
-        s_idx = np.asarray(inp["sensor_mask_index"], dtype=np.int64).ravel() - 1
+        s_idx = np.asarray(inp["sensor_mask_index"], dtype=np.int64).ravel() - 1 \
+            if inp.get("sensor_interp_index") is None else None
     else:
         s_idx = cuboid_mask_index(inp["sensor_mask_corners"], N).astype(np.int64) - 1
-    Ns = s_idx.size
+    # Cartesian points by linear interpolation: sum(field(tri) .* bc, 2)
+    # every step (kspaceFirstOrder_extractSensorData.m:296-420)
+    if inp.get("sensor_interp_index") is not None:
+        K = dim + 1
+        tri = np.asarray(inp["sensor_interp_index"], dtype=np.int64).reshape(-1, K) - 1
+        bc = np.asarray(inp["sensor_interp_weight"], dtype=np.float64).reshape(-1, K)
+
+        def at_sensors(f):
+            return np.sum(f.reshape(-1, order="F")[tri] * bc, axis=1).astype(rdt)
+        Ns = tri.shape[0]
+    else:
+        def at_sensors(f):
+            return f.reshape(-1, order="F")[s_idx]
+        Ns = s_idx.size
     start = int(record_start_index)
     n_rec = max(Nt - start + 1, 0)
     out = {}
@@ -386,7 +400,7 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
         # sensors (kspaceFirstOrder_extractSensorData.m:39-291,462-566)
         if t_index >= start:
             fi = t_index - start + 1
-            ps = flat(p)[s_idx]
+            ps = at_sensors(p)
             if "p" in record:
                 out["p"][:, fi - 1] = ps
             if "p_max" in record:
@@ -396,7 +410,7 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
             if "p_rms" in record:
                 out["p_rms"] = np.sqrt((out["p_rms"] ** 2 * (fi - 1) + ps ** 2) / fi).astype(rdt)
             for i, c in enumerate("xyz"[:dim]):
-                us = flat(u[i])[s_idx]
+                us = at_sensors(u[i])
                 if "u" in record:
                     out["u" + c][:, fi - 1] = us
                 if "u_max" in record:
@@ -412,7 +426,7 @@ def simulate(inp, record=("p",), record_start_index=1, dtype=np.float32, workers
                     sh = cast(op.shift_neg[i])
                     ush = sfft.ifft(sh * sfft.fft(u[i], axis=i, workers=workers), axis=i,
                                     workers=workers).real.astype(rdt)
-                    out["u" + c + "_non_staggered"][:, fi - 1] = flat(ush)[s_idx]
+                    out["u" + c + "_non_staggered"][:, fi - 1] = at_sensors(ush)
                 if "u_max_all" in record:
                     key = "u" + c + "_max_all"
                     out[key] = u[i].copy() if fi == 1 else np.maximum(out[key], u[i])

@@ -54,8 +54,9 @@ def test_points_outside_the_grid_are_rejected():
 
 
 def test_linear_sensor_outputs_through_the_oracle():
-    """Oracle run on the vertex set, then postprocess(): raw series are the
-    weighted vertex sums; max / min / rms are reductions of those series."""
+    """The point outputs are the weighted vertex sums each step, and max /
+    min / rms are reductions of those series: checked against a run that
+    records the vertices themselves as a binary mask."""
     from oracle.kspace_oracle import simulate
 
     n = (48, 40)
@@ -67,32 +68,42 @@ def test_linear_sensor_outputs_through_the_oracle():
     medium = {"sound_speed": 1500.0, "density": 1000.0}
     inp, record, start, meta = prepare(kg, medium, {"p0": p0}, {"mask": pts, "record": rec}, pml_size=6,
                                        cart_interp="linear")
-    assert sorted(record) == ["p", "u"] and meta["interp"]["w"].shape == (9, 3)
-    raw = simulate(inp, record=record, record_start_index=start, dtype=np.float64)
-    out = postprocess({k: v.copy() for k, v in raw.items()}, inp, meta)
+    assert record == rec and inp["sensor_interp_index"].shape == (9, 3)
+    out = postprocess(simulate(inp, record=record, record_start_index=start, dtype=np.float64), inp, meta)
     assert set(out) == {"p", "p_max", "p_min", "p_rms", "ux_max", "uy_max", "ux_rms", "uy_rms"}
-    col, w = meta["interp"]["col"], meta["interp"]["w"]
+    verts, w = inp["sensor_interp_index"], inp["sensor_interp_weight"]
+    uniq = np.unique(verts)
+    vin = dict(inp, sensor_mask_index=uniq)
+    vin.pop("sensor_interp_index")
+    vin.pop("sensor_interp_weight")
+    raw = simulate(vin, record=["p", "u"], dtype=np.float64)
+    col = np.searchsorted(uniq, verts)
     p = np.einsum("pj,pjt->pt", w, raw["p"][col])
-    np.testing.assert_allclose(out["p"], p, rtol=1e-6, atol=1e-9 * np.abs(p).max())
-    np.testing.assert_allclose(out["p_max"], p.max(axis=1), rtol=1e-6)
-    np.testing.assert_allclose(out["p_min"], p.min(axis=1), rtol=1e-6)
-    np.testing.assert_allclose(out["p_rms"], np.sqrt(np.mean(p * p, axis=1)), rtol=1e-6)
+    np.testing.assert_allclose(out["p"], p, rtol=1e-12, atol=1e-12 * np.abs(p).max())
+    np.testing.assert_allclose(out["p_max"], p.max(axis=1), rtol=1e-12)
+    np.testing.assert_allclose(out["p_min"], p.min(axis=1), rtol=1e-12)
+    np.testing.assert_allclose(out["p_rms"], np.sqrt(np.mean(p * p, axis=1)), rtol=1e-10)
     uy = np.einsum("pj,pjt->pt", w, raw["uy"][col])
-    np.testing.assert_allclose(out["uy_max"], uy.max(axis=1), rtol=1e-6)
+    np.testing.assert_allclose(out["uy_max"], uy.max(axis=1), rtol=1e-12)
     # against nearest-point recording of the same circle: same field, close values
     inp_n, record_n, _, meta_n = prepare(kg, medium, {"p0": p0}, {"mask": pts, "record": ["p"]}, pml_size=6)
     near = postprocess(simulate(inp_n, record=record_n, dtype=np.float64), inp_n, meta_n)
     assert np.max(np.abs(near["p"] - out["p"])) < 0.5 * np.abs(near["p"]).max()
 
 
-def test_linear_interp_sphere_vertex_count():
+def test_linear_interp_inputs_and_file_refusal(tmp_path):
+    from kwave import h5io
+
     kg = KWaveGrid((24, 24, 24), (1e-4, 1e-4, 1e-4))
     kg.set_time(10, 1e-8)
     pts = make_cart_sphere(8e-4, 30)
     inp, record, _, meta = prepare(kg, {"sound_speed": 1500.0}, {"p0": np.zeros(kg.N)},
                                    {"mask": pts, "record": ["p"]}, pml_size=4, cart_interp="linear")
-    idx = inp["sensor_mask_index"]
-    assert np.all(np.diff(idx) > 0) and len(idx) <= 4 * 30
-    np.testing.assert_array_equal(idx[meta["interp"]["col"]], cart_linear_weights(kg, pts)[0])
+    v, w = cart_linear_weights(kg, pts)
+    np.testing.assert_array_equal(inp["sensor_interp_index"], v)
+    np.testing.assert_allclose(inp["sensor_interp_weight"], w)
+    assert "sensor_mask_index" not in inp
+    with pytest.raises(ValueError, match="interpolated"):
+        h5io.write_input_file(tmp_path / "x.h5", inp)
     with pytest.raises(ValueError):
         prepare(kg, {"sound_speed": 1500.0}, {"p0": np.zeros(kg.N)}, {"mask": pts}, cart_interp="cubic")

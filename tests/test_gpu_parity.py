@@ -265,3 +265,26 @@ def test_3d_cartesian_linear_interpolation():
     assert set(tol) <= set(gpu) and gpu["p"].shape == (40, 70)
     bad = {k: rel_l2(gpu[k], ora[k]) for k in tol if not rel_l2(gpu[k], ora[k]) <= tol[k]}
     assert not bad, bad
+
+
+def test_2d_cartesian_circle_linear_interpolation():
+    """The 2D Cartesian-circle configuration (50 points, 'CartInterp' linear,
+    the in-memory default): per-point series and reductions formed on the
+    device each step; full-grid outputs alongside."""
+    from kwave import _lib
+    from kwave.simulation import postprocess, prepare
+    from kwave.utils import KWaveGrid, make_cart_circle, make_disc
+
+    n = (128, 128)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    kg.set_time(150, 0.3e-4 / 1500)
+    p0 = 5 * make_disc(*n, 64, 60, 5) + 3 * make_disc(*n, 50, 80, 4)
+    sensor = {"mask": make_cart_circle(4.5e-3, 50), "record": ["p", "p_max", "p_min", "p_rms", "u_rms", "u",
+                                                                 "p_final", "p_max_all"]}
+    inp, record, start, meta = prepare(kg, {"sound_speed": 1500.0, "density": 1000.0}, {"p0": p0}, sensor,
+                                       pml_size=20, cart_interp="linear")
+    gpu = postprocess(_lib.solve(inp, record=record, start_index=start), inp, meta)
+    ora = postprocess(oracle_outputs(inp, record, start, dtype=np.float64), inp, meta)
+    assert gpu["p"].shape == (50, 150) and gpu["p_max_all"].shape == n
+    bad = {k: rel_l2(gpu[k], ora[k]) for k in ora if not rel_l2(gpu[k], ora[k]) <= TOL_LOSSLESS}
+    assert not bad, bad

@@ -54,3 +54,21 @@ def test_streamed_series_3d_source():
     ns = full["p"].shape[0]
     streamed = _solve_with_budget(inp, record, 1, 4 * ns * 4 * 9 + 1)  # a ring of 9 steps
     _same(streamed, full)
+
+
+def test_streamed_interpolated_points():
+    """Cartesian points interpolated on the device stream like grid points."""
+    from kwave import _lib
+    from kwave.simulation import prepare
+    from kwave.utils import KWaveGrid, make_cart_circle, make_disc
+
+    kg = KWaveGrid((64, 64), (1e-4, 1e-4))
+    kg.set_time(60, 0.3e-4 / 1500)
+    record = ["p", "u", "u_non_staggered", "p_max"]
+    inp, record, start, _ = prepare(kg, {"sound_speed": 1500.0, "density": 1000.0},
+                                    {"p0": 2 * make_disc(64, 64, 32, 30, 4)},
+                                    {"mask": make_cart_circle(2e-3, 20), "record": record}, pml_size=8,
+                                    cart_interp="linear")
+    full = _lib.solve(inp, record, start_index=3)
+    streamed = _solve_with_budget(inp, record, 3, 4 * 20 * 5 * 6 + 1)  # a ring of 6 steps
+    _same(streamed, full)
