@@ -51,6 +51,57 @@ def gpu_session(inp, record, start_index=1, device=-1):
     return Session(inp, record, start_index, device)
 
 
+BINARY = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "kspaceFirstOrder-B200")
+_FLAGS = {"p": "--p_raw", "u": "--u_raw", "u_non_staggered": "--u_non_staggered_raw"}
+
+
+class DropInSession:
+    """One solve the way the reference's C/G-suffixed wrappers run it
+    (kspaceFirstOrder3DC.m:159-212, 462-545, 569-776): the input file
+    written, the solver binary started, the output file read.  The session
+    interface of :func:`gpu_session`, so the plain one-solve-at-a-time
+    drop-in can be timed with the same schedulers: ``advance`` runs the
+    whole solve."""
+
+    def __init__(self, inp, record, start_index=1, device=-1, workdir=None):
+        import tempfile
+
+        self.inp, self.record, self.start, self.device = inp, tuple(record), int(start_index), device
+        self.dir = tempfile.mkdtemp(prefix="kwb_dropin_", dir=workdir)
+        self.result = None
+
+    def advance(self, n):
+        import subprocess
+
+        from . import h5io
+
+        fin, fout = os.path.join(self.dir, "input.h5"), os.path.join(self.dir, "output.h5")
+        h5io.write_input_file(fin, self.inp)
+        cmd = [BINARY, "-i", fin, "-o", fout, "-s", str(self.start)]
+        cmd += [_FLAGS.get(r, "--" + r) for r in self.record]
+        if self.device >= 0:
+            cmd += ["-g", str(self.device)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"drop-in binary failed ({r.returncode}): {r.stderr.strip()}")
+        self.result = h5io.read_output_file(fout, 2 if int(self.inp["Nz"]) == 1 else 3)
+
+    def sync(self):
+        pass
+
+    def read(self):
+        return self.result
+
+    def close(self):
+        import shutil
+
+        shutil.rmtree(self.dir, ignore_errors=True)
+
+
+def dropin_session(inp, record, start_index=1, device=-1):
+    return DropInSession(inp, record, start_index, device)
+
+
 @dataclass
 class Request:
     """One simulation request: the input datasets, what to record, and when

@@ -88,3 +88,18 @@ def test_in_flight_reports_running_chunks():
         assert s.in_flight() == 0
     finally:
         s.close()
+
+
+def test_dropin_sessions_give_the_same_results():
+    """The plain drop-in baseline (solver binary per request, files in and
+    out) returns what the resident sessions return, bit for bit."""
+    from kwave import serving
+
+    cases = _cases()[:3]
+    reqs = [serving.Request(inp=inp, record=rec, arrival=0.0, tag=i) for i, (inp, rec) in enumerate(cases)]
+    dropped = serving.serve_plain(reqs, factory=serving.dropin_session)
+    for r, (inp, rec) in zip(dropped, cases):
+        s = serving.gpu_session(inp, rec)
+        s.advance(int(inp["Nt"]))
+        _same(r.result, s.read())
+        s.close()
