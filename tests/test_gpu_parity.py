@@ -288,3 +288,24 @@ def test_2d_cartesian_circle_linear_interpolation():
     assert gpu["p"].shape == (50, 150) and gpu["p_max_all"].shape == n
     bad = {k: rel_l2(gpu[k], ora[k]) for k in ora if not rel_l2(gpu[k], ora[k]) <= TOL_LOSSLESS}
     assert not bad, bad
+
+
+@pytest.mark.parametrize("interp", ["linear", "nearest"])
+def test_config_2d_two_discs_cartesian_circle(interp):
+    """The reference's CPU-runnable case: 128 x 128, dx 0.1 mm, lossless
+    homogeneous, PML 20, two smoothed discs of p0, a 50-point Cartesian circle
+    of radius 4 mm (linear: the in-memory default; nearest: the file path),
+    CFL 0.3 to 8 us."""
+    from kwave import _lib
+    from kwave.simulation import postprocess, prepare
+    from kwave.workloads import two_disc_2d
+
+    kg, medium, source, sensor = two_disc_2d()
+    sensor["record"] = ["p", "p_max", "p_rms"]
+    inp, record, start, meta = prepare(kg, medium, source, sensor, cart_interp=interp)
+    assert inp["Nt"] == kg.Nt and kg.Nt > 300
+    gpu = postprocess(_lib.solve(inp, record=record, start_index=start), inp, meta)
+    ora = postprocess(oracle_outputs(inp, record, start, dtype=np.float64), inp, meta)
+    assert gpu["p"].shape == (50, kg.Nt)
+    bad = {k: rel_l2(gpu[k], ora[k]) for k in ora if not rel_l2(gpu[k], ora[k]) <= TOL_LOSSLESS}
+    assert not bad, bad
