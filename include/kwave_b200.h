@@ -133,8 +133,9 @@ typedef struct {
    * Axisymmetric simulation (kspaceFirstOrderAS.m; saveToDisk.m:90-100, 125):
    * x axial, y radial with the axis at y = 0, Nz = 1.  Medium, p0 and source
    * positions are given on the Nx x Ny grid; the radial PML sits at the
-   * outer radius only.  Initial pressure and pressure sources, lossless or
-   * Stokes media (absorbing_flag 0 or 2), with or without B/A.
+   * outer radius only.  Initial pressure, pressure sources and axial (x)
+   * velocity sources, lossless or Stokes media (absorbing_flag 0 or 2), with
+   * or without B/A.
    */
   uint64_t axisymmetric_flag;
 

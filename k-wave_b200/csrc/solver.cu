@@ -228,8 +228,8 @@ const kw_input* Session::expand_axisymmetric(const kw_input* in) {
   if (in->Nz != 1) throw KwError(KW_ERR_INVALID_ARGUMENT, "axisymmetric grids are 2D (Nz must be 1)");
   if (in->absorbing_flag == 1)
     throw KwError(KW_ERR_UNSUPPORTED, "axisymmetric simulations take Stokes absorption only (absorbing_flag 2)");
-  if (in->ux_source_flag || in->uy_source_flag || in->uz_source_flag || in->transducer_source_flag)
-    throw KwError(KW_ERR_UNSUPPORTED, "velocity and transducer sources are not supported on axisymmetric grids");
+  if (in->uy_source_flag || in->uz_source_flag || in->transducer_source_flag)
+    throw KwError(KW_ERR_UNSUPPORTED, "radial velocity and transducer sources are not supported on axisymmetric grids");
   if (opt.u_non_staggered_raw)
     throw KwError(KW_ERR_UNSUPPORTED, "u_non_staggered_raw is not supported on axisymmetric grids");
   if (in->Ny < 2 || in->Nx < 1) throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx and Ny must be positive");
@@ -277,24 +277,36 @@ const kw_input* Session::expand_axisymmetric(const kw_input* in) {
       for (uint64_t x = 0; x < nx; ++x) asx.p0[x + nx * j] = ps[j] * in->p0_source_input[x + nx * pc[j]];
     asx.in.p0_source_input = asx.p0.data();
   }
-  p_rows0 = in->p_source_index_numel;
-  if (in->p_source_flag && in->p_source_index) {
-    // each source point and its mirror images, with the sign of the pressure there
-    for (uint64_t e = 0; e < in->p_source_index_numel; ++e) {
-      const uint64_t lin = in->p_source_index[e];
-      if (lin < 1 || lin > nx * ny) throw KwError(KW_ERR_INVALID_ARGUMENT, "p_source_index holds an index outside the grid");
+  // source points and their mirror images, with the sign of the field there:
+  // pressure and the axial velocity follow the pressure-point pattern
+  // (kspaceFirstOrderAS.m:795-798, 1041-1044)
+  auto mirror_points = [&](const uint64_t* idx, uint64_t n, std::vector<uint64_t>& out, std::vector<int>& orig,
+                           std::vector<float>& w, const char* name) {
+    for (uint64_t e = 0; e < n; ++e) {
+      const uint64_t lin = idx[e];
+      if (lin < 1 || lin > nx * ny) throw KwError(KW_ERR_INVALID_ARGUMENT, std::string(name) + " holds an index outside the grid");
       const uint64_t x = (lin - 1) % nx, y = (lin - 1) / nx;
       const uint64_t cols[4] = {y, 2 * ny - y, 2 * ny + y, 4 * ny - y};
       const float sg[4] = {1.f, -1.f, -1.f, 1.f};
       for (int k = 0; k < 4; ++k) {
         if ((k == 1 || k == 3) && y == 0) continue;
-        asx.p_idx.push_back(x + nx * cols[k] + 1);
-        asx.p_orig.push_back((int)e);
-        asx.p_w.push_back(sg[k]);
+        out.push_back(x + nx * cols[k] + 1);
+        orig.push_back((int)e);
+        w.push_back(sg[k]);
       }
     }
+  };
+  p_rows0 = in->p_source_index_numel;
+  if (in->p_source_flag && in->p_source_index) {
+    mirror_points(in->p_source_index, in->p_source_index_numel, asx.p_idx, asx.p_orig, asx.p_w, "p_source_index");
     asx.in.p_source_index = asx.p_idx.data();
     asx.in.p_source_index_numel = asx.p_idx.size();
+  }
+  u_rows0 = in->u_source_index_numel;
+  if (in->ux_source_flag && in->u_source_index) {
+    mirror_points(in->u_source_index, in->u_source_index_numel, asx.u_idx, asx.u_orig, asx.u_w, "u_source_index");
+    asx.in.u_source_index = asx.u_idx.data();
+    asx.in.u_source_index_numel = asx.u_idx.size();
   }
   if (in->sensor_mask_type == 0) {
     for (uint64_t j = 0; j < in->sensor_mask_index_numel; ++j)
@@ -319,6 +331,7 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   if (in->Nx < 1 || in->Ny < 1 || in->Nz < 1 || in->Nt < 1)
     throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
   p_rows0 = in->p_source_index_numel;
+  u_rows0 = in->u_source_index_numel;
   if (in->axisymmetric_flag) in = expand_axisymmetric(in);
   if (in->Ny == 1) throw KwError(KW_ERR_UNSUPPORTED, "1D simulations are not supported (Ny must be > 1)");
   for (uint64_t n : {in->Nx, in->Ny, in->Nz}) {
@@ -661,9 +674,18 @@ void Session::setup_sources(const kw_input* in) {
       throw KwError(KW_ERR_INVALID_ARGUMENT, "u_source_index missing");
     std::vector<int> si, sl;
     sort_indices(in->u_source_index, in->u_source_index_numel, d.npts, si, sl, "u_source_index");
-    const int nsig = in->u_source_many ? (int)in->u_source_index_numel : 1;
+    const int nsig = in->u_source_many ? (int)u_rows0 : 1;
     u_mode = (int)in->u_source_mode;
     if (u_mode < 0 || u_mode > 2) throw KwError(KW_ERR_INVALID_ARGUMENT, "u_source_mode must be 0, 1 or 2");
+    const float* duw = nullptr;
+    if (axisym) {
+      std::vector<float> w(sl.size());
+      for (size_t j = 0; j < sl.size(); ++j) {
+        w[j] = asx.u_w[sl[j]];
+        sl[j] = asx.u_orig[sl[j]];
+      }
+      duw = up(usrc_w, w.data(), w.size(), st);
+    }
     const int* didx = up(usrc_idx, si.data(), si.size(), st);
     const int* dslot = up(usrc_slot, sl.data(), sl.size(), st);
     u_nsrc = (int)si.size();
@@ -684,7 +706,7 @@ void Session::setup_sources(const kw_input* in) {
           if (!ones_ready) {
             std::vector<float> ones(1, 1.0f);
             const float* d1 = up(ones_buf, ones.data(), 1, st);
-            corrected_source((float*)ufield_buf[a].p, didx, dslot, u_nsrc, d1, 1, 1);
+            corrected_source((float*)ufield_buf[a].p, didx, dslot, u_nsrc, d1, 1, 1, duw);
             ones_ready = true;
             ones_field = a;
           } else {
@@ -704,6 +726,7 @@ void Session::setup_sources(const kw_input* in) {
       usrc.nrows_sig = nsig;
       usrc.mode = u_mode;
       usrc.len = 0;
+      usrc.weight = duw;
     }
   }
   // transducer source (kspaceFirstOrder_inputChecking.m:1155-1213 builds
@@ -1217,7 +1240,7 @@ void Session::enqueue_step_body(uint64_t t) {
         if (udense[a].field && (int)t <= u_len[a]) {
           // S0 is free here: the gradient has been taken
           corrected_source_into((float*)ufield_buf[a].p, (const int*)usrc_idx.p, (const int*)usrc_slot.p, u_nsrc,
-                                usig_d[a], u_nsig, (int)t, 0);
+                                usig_d[a], u_nsig, (int)t, 0, (const float*)usrc_w.p);
         }
     }
     UArgs ua = u_args(S);

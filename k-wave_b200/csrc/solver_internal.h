@@ -123,12 +123,12 @@ class Session {
   struct AxisymmetricInput {
     kw_input in;
     std::vector<float> c0, rho0, sgx, sgy, bona, alpha, p0;
-    std::vector<uint64_t> p_idx;
-    std::vector<int> p_orig;
-    std::vector<float> p_w;
+    std::vector<uint64_t> p_idx, u_idx;
+    std::vector<int> p_orig, u_orig;
+    std::vector<float> p_w, u_w;
   } asx;
-  uint64_t p_rows0 = 0;  // pressure-source points before mirroring
-  DevBuf psrc_w, inv_r_buf, ur_buf;
+  uint64_t p_rows0 = 0, u_rows0 = 0;  // source points before mirroring
+  DevBuf psrc_w, usrc_w, inv_r_buf, ur_buf;
   // TMA tensor maps over the half-spectrum buffers (y pass / z pass)
   bool use_tma[3]{false, false, false};
   CUtensorMap map_y[5], map_z[5];  // [4]: the axisymmetric u_r / r spectrum

@@ -146,8 +146,8 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
             raise NotImplementedError("PMLInside = false is not supported for axisymmetric simulations")
         if isinstance(source, KWaveTransducer) or isinstance(sensor, KWaveTransducer):
             raise ValueError("Transducer inputs are only compatible with 3D simulations.")
-        if any(k in source for k in ("ux", "uy", "u_mask")):
-            raise NotImplementedError("velocity sources are not supported for axisymmetric simulations")
+        if "uy" in source:
+            raise NotImplementedError("radial velocity sources are not supported for axisymmetric simulations")
     dim = kgrid.dim
     if kgrid.dt is None or kgrid.Nt is None:
         kgrid.make_time(medium["sound_speed"])

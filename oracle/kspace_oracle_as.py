@@ -2,9 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY, like ``kspace_oracle.py``: only ``tests/`` may use
 it, as the checker.  Parity status: UNPINNED against outputs of the reference
-(MATLAB); pinned here against the reference's own statement that its DTT and
-FFT forms of the radial symmetry agree, and against the 2D loop for fields
-far from the axis (``tests/test_oracle_as.py``).
+(MATLAB); pinned instead against the 3D loop run on a rotationally symmetric
+field (``tests/test_oracle_as.py``): two discretisations of one problem.
 
 The restatement follows the default radial symmetry 'WSWA-FFT': each step
 the pressure and velocity fields (x axial, y radial from the axis, grid
@@ -14,10 +13,10 @@ differentiated there with the ordinary staggered k-space operators, and cut
 back to the first Ny columns.  The radial divergence carries the extra
 u_r / r term (``kspaceFirstOrderAS.m:930-934``); the radial PML sits at the
 outer radius only (``private/getPML.m:74-77``).  Supported: initial
-pressure, pressure sources (dirichlet, additive, additive without
-correction), lossless and Stokes media with or without B/A, binary sensor
-masks recording p and u (time series, max / min / rms, full-grid max / min
-/ final).  Inputs are the datasets of the input file, on the Nx x Ny grid.
+pressure, pressure and axial velocity sources (dirichlet, additive,
+additive without correction), lossless and Stokes media with or without
+B/A, binary sensor masks recording p and u (time series, max / min / rms,
+full-grid max / min / final).  Inputs are the datasets of the input file, on the Nx x Ny grid.
 """
 from __future__ import annotations
 
@@ -126,9 +125,15 @@ def simulate_as(inp, record=("p",), record_start_index=1, dtype=np.float32, work
         p_idx = np.asarray(inp["p_source_index"], dtype=np.int64).ravel() - 1
         p_sig = np.asarray(inp["p_source_input"], dtype=np.float64)
         p_sig = p_sig.reshape(-1, p_sig.shape[-1]).astype(rdt)
-    for c in "xyz":
+    for c in "yz":
         if int(inp.get(f"u{c}_source_flag", 0)):
-            raise NotImplementedError("velocity sources are not restated for the axisymmetric loop")
+            raise NotImplementedError("radial velocity sources are not restated for the axisymmetric loop")
+    ux_flag = int(inp.get("ux_source_flag", 0))
+    if ux_flag:
+        u_mode = int(inp["u_source_mode"])
+        u_idx = np.asarray(inp["u_source_index"], dtype=np.int64).ravel() - 1
+        ux_sig = np.asarray(inp["ux_source_input"], dtype=np.float64)
+        ux_sig = ux_sig.reshape(-1, ux_sig.shape[-1]).astype(rdt)
     p0_flag = int(inp.get("p0_source_flag", 0)) != 0
     if p0_flag:
         p0 = np.asarray(inp["p0_source_input"], dtype=np.float64).reshape(nd, order="F").astype(rdt)
@@ -172,6 +177,16 @@ def simulate_as(inp, record=("p",), record_start_index=1, dtype=np.float32, work
         dpdx, dpdy = grad(p)
         ux = pml_x_sg * (pml_x_sg * ux - dt * rinv_x * dpdx)
         uy = pml_y_sg * (pml_y_sg * uy - dt * rinv_y * dpdy)
+        # axial velocity source (:785-830), mirrored like the pressure
+        if ux_flag >= t_index:
+            v = sig_at(ux_sig, t)
+            if u_mode == 0:
+                ux = scatter(ux, u_idx, v, False)
+            elif u_mode == 2:
+                sm = scatter(np.zeros(nd, rdt), u_idx, v, False)
+                ux = ux + ifft2r(source_kappa * fft2(mirror_p(sm, Ny)))[:, :Ny]
+            else:
+                ux = scatter(ux, u_idx, v, True)
         # divergence with the u_r / r term (:905-935)
         duxdx = ifft2r(ddx_neg * (kappa * fft2(mirror_p(ux, Ny))))[:, :Ny]
         duydy = ifft2r(kappa * (y_neg * (ddy * fft2(mirror_sg(uy, Ny)) +

@@ -137,3 +137,19 @@ def test_tester_axisymmetric_case():
     ora = postprocess(simulate_as(inp, record=record, record_start_index=start, dtype=np.float64), inp, meta)
     errs = {k: rel_l2(gpu[k], ora[k]) for k in ora}
     assert max(errs.values()) <= TOL, errs
+
+
+@pytest.mark.parametrize("mode", [2, 1, 0])
+def test_axial_velocity_sources(mode):
+    """A piston: axial velocity on a disc of the axial plane, the usual
+    axisymmetric transducer model (kspaceFirstOrderAS.m:785-830)."""
+    base = _inputs(64, 32, 60, het=True)
+    base.update(p0_source_flag=0)
+    t = np.arange(35) * base["dt"]
+    sig = 1e-3 * np.sin(2 * np.pi * 2e6 * t) * np.hanning(35)
+    idx = np.array([10 + 64 * y for y in range(6)]) + 1  # x = 10, radius 0..5 (the axis included)
+    many = 1 if mode == 1 else 0
+    s = sig[None, :] * (1 + 0.1 * np.arange(6)[:, None]) if many else sig[None, :]
+    base.update(ux_source_flag=35, u_source_mode=mode, u_source_many=many, u_source_index=idx, ux_source_input=s)
+    gpu = _check(base, ("p", "u", "p_max", "p_final"), TOL)
+    assert np.abs(gpu["p"]).max() > 0

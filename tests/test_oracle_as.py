@@ -94,6 +94,9 @@ def test_front_end_builds_axisymmetric_datasets():
     m[:, 40:60] = -p0
     m[:, 61:] = p0[:, 1:][:, ::-1]
     np.testing.assert_allclose(np.asarray(inp["p0_source_input"]).reshape(40, 20), smooth(m, True)[:, :20])
-    with pytest.raises(NotImplementedError):
-        prepare(kg, {"sound_speed": 1500.0}, {"u_mask": np.ones((40, 20)), "ux": np.ones((1, 5))},
+    with pytest.raises(NotImplementedError):  # radial velocity sources
+        prepare(kg, {"sound_speed": 1500.0}, {"u_mask": np.ones((40, 20)), "uy": np.ones((1, 5))},
                 {"mask": np.ones((40, 20))}, pml_size=5, axisymmetric=True)
+    ux, _, _, _ = prepare(kg, {"sound_speed": 1500.0}, {"u_mask": np.ones((40, 20)), "ux": np.ones((1, 5))},
+                          {"mask": np.ones((40, 20))}, pml_size=5, axisymmetric=True)
+    assert ux["ux_source_flag"] == 5 and ux["axisymmetric_flag"] == 1
