@@ -39,12 +39,20 @@ __device__ __forceinline__ void tile_coords(int yaxis, int cx, int o, int lines,
   }
 }
 
+// Shared-memory stages of the y pass: tiles t + grid and t + 2 grid load
+// while tile t is transformed and stored.  With two stages the refill of a
+// stage waits for the store out of it to have read it.
+#ifndef KWB_COL_STAGES
+#define KWB_COL_STAGES 3
+#endif
+constexpr int kColStages = KWB_COL_STAGES;
+
 template <int NC, bool INV>
 __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_constant__ ColTmaArgs a,
                                                                 const float2* __restrict__ tw_g) {
   constexpr int TL = TTile<NC>::LINES;
   constexpr int E = TTile<NC>::ELEMS;
-  constexpr int ST = 3;
+  constexpr int ST = kColStages;
   extern __shared__ __align__(128) unsigned char smraw[];
   float2* bufs = reinterpret_cast<float2*>(smraw);
   float2* tw = bufs + ST * E;
@@ -90,7 +98,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
       bulk_commit();
       const int t2 = t + 2 * gridDim.x;
       if (t2 < ntiles) {
-        bulk_wait_read<1>();  // the stage being refilled was stored one tile ago
+        bulk_wait_read<ST - 2>();  // the store out of the stage being refilled has read it
         issue(t2, (it + 2) % ST);
       }
     }
@@ -102,10 +110,12 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
 // only that operator's arithmetic in the kernel body.
 enum FusedClass { FC_GRAD = 0, FC_NABLA = 1, FC_SRCK = 2 };
 
-// ONE: every input has a single output (the register hand-off path);
-// otherwise the forward transform is kept and each output multiplied from it.
+// ONE: every input has a single output (the register hand-off path, in
+// place in the input stage: two tile buffers, three blocks per SM);
+// otherwise the forward transform is kept and each output multiplied from it
+// into a third buffer (two blocks per SM).
 template <int NC, int CLS, bool ONE>
-__global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
+__global__ void __launch_bounds__(TTile<NC>::THREADS, ONE ? 3 : 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
                                                                      const float2* __restrict__ tw_g,
                                                                      const __grid_constant__ SpecTables T) {
   constexpr int TL = TTile<NC>::LINES;
@@ -114,8 +124,8 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
   static_assert(Ct<NC>::S == 2, "the fused last-axis kernel assumes a two-stage plan");
   extern __shared__ __align__(128) unsigned char smraw[];
   float2* inb = reinterpret_cast<float2*>(smraw);  // 2 input stages
-  float2* W = inb + 2 * E;                         // product / inverse-transform buffer
-  float2* tw = W + E;
+  float2* W = ONE ? nullptr : inb + 2 * E;         // product / inverse-transform buffer (fanout > 1)
+  float2* tw = inb + (ONE ? 2 : 3) * E;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + NC);
   // per-line tables of the transform axis: shifted derivatives (+, -) and k^2
   float2* dpos = reinterpret_cast<float2*>(bar + 2);
@@ -221,7 +231,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
     };
     // inverse last stage, straight from W to the output (and the optional
     // second output scaled by a factor constant along the line)
-    auto finish = [&](int q) {
+    auto finish = [&](int q, const float2* src) {
       float2* dst = a.outp[g * a.fanout + q] + (long long)o * a.ostride + x0;
       float2* dst2 = a.dual_outp[g * a.fanout + q];
       float2 dsc = make_float2(0.f, 0.f);
@@ -230,7 +240,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
         dsc = __ldg(a.dual_tab[g * a.fanout + q] + o);
       }
       const bool valid = (x0 + l) < a.ncols;
-      auto ld_w = [&](int ll, int pos) -> float2 { return W[lay(ll, pos)]; };
+      auto ld_w = [&](int ll, int pos) -> float2 { return src[lay(ll, pos)]; };
       auto st_g = [&](int ll, int pos, float2 v) {
         if (valid) {
           dst[pos * a.lstride + ll] = v;
@@ -238,7 +248,8 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
         }
       };
       ct_stage_io<NC, 1, true>(tw, l, tid, ld_w, st_g);
-      __syncthreads();  // W is reused by the next inverse
+      fence_async_smem();  // the reads of src come before a TMA refill of it
+      __syncthreads();     // src is reused by the next inverse
     };
     auto refill = [&]() {  // F is consumed: refill this input stage with the tile two ahead
       if (threadIdx.x == 0) {
@@ -250,15 +261,17 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
     if constexpr (ONE) {
       float2 u[M];
       // forward first stage in place; last stage, operator and inverse first
-      // stage in registers; inverse last stage to the output
+      // stage in registers, the latter's outputs back into F once every
+      // thread has read its inputs; inverse last stage to the output; then F
+      // takes the tile two ahead
       ct_stage<NC, 0, false>(F, tw, l, tid, lay);
       ct_fwd_last_to_regs<NC>(F, tw, l, tid, lay, u);
       apply(setup(0), u);
-      ct_inv_first_from_regs<NC>(u, W, l, tid, lay);
-      fence_async_smem();
       __syncthreads();
+      ct_inv_first_from_regs<NC>(u, F, l, tid, lay);
+      __syncthreads();
+      finish(0, F);
       refill();
-      finish(0);
     } else {
       // several outputs of one input: the forward transform stays in F; each
       // output is read from it in the hand-off order, multiplied in registers
@@ -274,7 +287,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, 2) k_fused_tma(const __gri
         if (q + 1 == a.fanout) fence_async_smem();
         __syncthreads();
         if (q + 1 == a.fanout) refill();
-        finish(q);
+        finish(q, W);
       }
     }
   }
@@ -329,7 +342,7 @@ static int num_sms() {
 
 template <int NC, bool INV>
 static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t st) {
-  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 3 * sizeof(uint64_t);
+  const size_t sm = kColStages * TTile<NC>::BYTES + NC * sizeof(float2) + kColStages * sizeof(uint64_t);
   auto k = k_col_tma<NC, INV>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;
@@ -342,7 +355,7 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
 
 template <int NC, int CLS, bool ONE>
 static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
-  const size_t sm = 3 * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
+  const size_t sm = (ONE ? 2 : 3) * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
                     NC * sizeof(float);
   auto k = k_fused_tma<NC, CLS, ONE>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
