@@ -108,12 +108,15 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
 // only that operator's arithmetic in the kernel body.
 enum FusedClass { FC_GRAD = 0, FC_NABLA = 1, FC_SRCK = 2 };
 
-// ONE: every input has a single output (the register hand-off path, in
-// place in the input stage: two tile buffers, three blocks per SM);
-// otherwise the forward transform is kept and each output multiplied from it
-// into a third buffer (two blocks per SM).
-template <int NC, int CLS, bool ONE>
-__global__ void __launch_bounds__(TTile<NC>::THREADS, ONE ? 3 : 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
+// MODE 1: every input has a single output (the register hand-off path, in
+// place in the input stage: two tile buffers, three blocks per SM).
+// MODE 0: the forward transform is kept and each output multiplied from it
+// into a third buffer (two blocks per SM).  (The gradient's pair of outputs,
+// kappa and kappa times the transform axis' derivative, also fits the
+// in-place form with both taken from the hand-off registers, but at three
+// blocks per SM that spills and measured slower: 1.338 against 1.330 ms.)
+template <int NC, int CLS, int MODE>
+__global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
                                                                      const float2* __restrict__ tw_g,
                                                                      const __grid_constant__ SpecTables T) {
   constexpr int TL = TTile<NC>::LINES;
@@ -122,8 +125,8 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, ONE ? 3 : 2) k_fused_tma(c
   static_assert(Ct<NC>::S == 2, "the fused last-axis kernel assumes a two-stage plan");
   extern __shared__ __align__(128) unsigned char smraw[];
   float2* inb = reinterpret_cast<float2*>(smraw);  // 2 input stages
-  float2* W = ONE ? nullptr : inb + 2 * E;         // product / inverse-transform buffer (fanout > 1)
-  float2* tw = inb + (ONE ? 2 : 3) * E;
+  float2* W = MODE ? nullptr : inb + 2 * E;        // product / inverse-transform buffer (MODE 0)
+  float2* tw = inb + (MODE ? 2 : 3) * E;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + NC);
   // per-line tables of the transform axis: shifted derivatives (+, -) and k^2
   float2* dpos = reinterpret_cast<float2*>(bar + 2);
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, ONE ? 3 : 2) k_fused_tma(c
       }
     };
     mbar_wait(&bar[s], (it >> 1) & 1, a.err);
-    if constexpr (ONE) {
+    if constexpr (MODE == 1) {
       float2 u[M];
       // forward first stage in place; last stage, operator and inverse first
       // stage in registers, the latter's outputs back into F once every
@@ -351,11 +354,11 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
   return cudaGetLastError();
 }
 
-template <int NC, int CLS, bool ONE>
+template <int NC, int CLS, int MODE>
 static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
-  const size_t sm = (ONE ? 2 : 3) * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
+  const size_t sm = (MODE ? 2 : 3) * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
                     NC * sizeof(float);
-  auto k = k_fused_tma<NC, CLS, ONE>;
+  auto k = k_fused_tma<NC, CLS, MODE>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
@@ -370,11 +373,12 @@ static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const 
   const int kind = a.op[0].kind;
   const bool one = a.fanout == 1;
   if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA || kind == OP_SHIFT_NEG ||
-      kind == OP_KAPPA_SHIFT_NEG)
-    return one ? fused_tma_t<NC, FC_GRAD, true>(a, tw, T, st) : fused_tma_t<NC, FC_GRAD, false>(a, tw, T, st);
+      kind == OP_KAPPA_SHIFT_NEG) {
+    return one ? fused_tma_t<NC, FC_GRAD, 1>(a, tw, T, st) : fused_tma_t<NC, FC_GRAD, 0>(a, tw, T, st);
+  }
   if (kind == OP_NABLA1 || kind == OP_NABLA2)
-    return one ? fused_tma_t<NC, FC_NABLA, true>(a, tw, T, st) : fused_tma_t<NC, FC_NABLA, false>(a, tw, T, st);
-  return one ? fused_tma_t<NC, FC_SRCK, true>(a, tw, T, st) : fused_tma_t<NC, FC_SRCK, false>(a, tw, T, st);
+    return one ? fused_tma_t<NC, FC_NABLA, 1>(a, tw, T, st) : fused_tma_t<NC, FC_NABLA, 0>(a, tw, T, st);
+  return one ? fused_tma_t<NC, FC_SRCK, 1>(a, tw, T, st) : fused_tma_t<NC, FC_SRCK, 0>(a, tw, T, st);
 }
 
 int tma_lines(int n) { return ct_lines_of(n); }
