@@ -570,16 +570,29 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;
   }
   // z slabs of the y-inverse / row kernel / y-forward chains.  Measured on
-  // 256^3: whole-volume launches (one slab) are fastest -- the per-slab
-  // launches lose more to partial waves than L2 reuse of the slab's half
-  // spectra gains -- so one slab is the default; KWAVE_B200_SLAB sets the
-  // planes per slab.
+  // 256^3: run one after another, slabs lose more to partial waves than L2
+  // reuse of a slab's half spectra gains (two slabs: 1.406 against 1.340 ms
+  // per step), but two slabs on two streams let one slab's latency-bound row
+  // kernel run beside the other's bandwidth-bound y passes (1.299 ms; four
+  // slabs 1.347).  So large 3D grids (2^22 points and more) take two slabs
+  // on two streams, others one slab.  KWAVE_B200_SLAB sets the planes per
+  // slab, KWAVE_B200_SLAB_STREAMS 1 or 2 the streams.
   {
-    int zs = d.nz;
+    const bool big = d.dim == 3 && d.npts >= (1LL << 22) && d.nz >= 64;
+    int zs = big ? (d.nz + 1) / 2 : d.nz;
     const char* env = std::getenv("KWAVE_B200_SLAB");
     if (env && std::atoi(env) > 0) zs = std::min(std::atoi(env), d.nz);
     const int nslab = (d.nz + zs - 1) / zs;
     slab = (d.nz + nslab - 1) / nslab;
+    const char* two = std::getenv("KWAVE_B200_SLAB_STREAMS");
+    const int nst = (two && std::atoi(two) > 0) ? std::atoi(two) : (big ? 2 : 1);
+    if (nslab > 1 && nst >= 2) {
+      int lo = 0, hi = 0;
+      cudaDeviceGetStreamPriorityRange(&lo, &hi);
+      ck(cudaStreamCreateWithPriority(&st2, cudaStreamNonBlocking, lo), "cudaStreamCreate");
+      ck(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming), "cudaEventCreate");
+      ck(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming), "cudaEventCreate");
+    }
   }
   if (eos == 1) ploc_buf.alloc(fb, st);
   if (opt.p_final) {
@@ -890,6 +903,25 @@ void Session::grad_pass() {
     fused_pass({0}, {1, 3}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 2}}, 2, {2, -1}, T.ddk_pos[1]);
   else
     fused_pass({0}, {1, 2}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 1}}, 2);
+}
+
+template <class F>
+void Session::for_slabs(F&& body) {
+  if (!st2) {
+    for (int z0 = 0; z0 < d.nz; z0 += slab) body(z0, std::min(slab, d.nz - z0));
+    return;
+  }
+  cudaStream_t main = st;
+  ck(cudaEventRecord(fork_ev, main), "fork");
+  ck(cudaStreamWaitEvent(st2, fork_ev, 0), "fork");
+  int k = 0;
+  for (int z0 = 0; z0 < d.nz; z0 += slab, ++k) {
+    st = (k % 2) ? st2 : main;
+    body(z0, std::min(slab, d.nz - z0));
+  }
+  st = main;
+  ck(cudaEventRecord(join_ev, st2), "join");
+  ck(cudaStreamWaitEvent(main, join_ev, 0), "join");
 }
 
 Dims Session::slab_dims(int z0, int nzs) const {
@@ -1244,13 +1276,12 @@ void Session::enqueue_step_body(uint64_t t) {
         }
     }
     UArgs ua = u_args(S);
-    for (int z0 = 0; z0 < d.nz; z0 += slab) {
-      const int nzs = std::min(slab, d.nz - z0);
+    for_slabs([&](int z0, int nzs) {
       col_pass(true, f123, z0, nzs);
       ck(launch_x_u(ua, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_u");
       ++launches_;
       col_pass(false, f123, z0, nzs);
-    }
+    });
     if (axisym) {
       // the radial term of the divergence: u_r / r, transformed along x
       // (kspaceFirstOrderAS.m:920-934)
@@ -1303,8 +1334,7 @@ void Session::enqueue_step_body(uint64_t t) {
       ra.p_out = last ? (float*)p_buf.p : nullptr;
       ra.S_p = S[0];
     }
-    for (int z0 = 0; z0 < d.nz; z0 += slab) {
-      const int nzs = std::min(slab, d.nz - z0);
+    for_slabs([&](int z0, int nzs) {
       col_pass(true, f123, z0, nzs);
       ck(launch_x_rho(ra, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_rho");
       ++launches_;
@@ -1312,7 +1342,7 @@ void Session::enqueue_step_body(uint64_t t) {
         col_pass(false, f12, z0, nzs);
       else
         col_pass(false, {0}, z0, nzs);
-    }
+    });
     if (eos != 1) interp_points(0);
     if (eos == 1) {
       // (3) power-law absorption and dispersion (:970-977)
@@ -1327,13 +1357,12 @@ void Session::enqueue_step_body(uint64_t t) {
       ea.S_p = S[0];
       ea.sens = row_sens_p();
       ea.clk = clk;
-      for (int z0 = 0; z0 < d.nz; z0 += slab) {
-        const int nzs = std::min(slab, d.nz - z0);
+      for_slabs([&](int z0, int nzs) {
         col_pass(true, f12, z0, nzs);
         ck(launch_x_eos(ea, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_eos");
         ++launches_;
         col_pass(false, {0}, z0, nzs);
-      }
+      });
       interp_points(0);
     }
   }
@@ -1573,6 +1602,12 @@ Session::~Session() {
   if (graph) cudaGraphDestroy(graph);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (st2) {
+    cudaStreamSynchronize(st2);
+    cudaStreamDestroy(st2);
+  }
+  if (fork_ev) cudaEventDestroy(fork_ev);
+  if (join_ev) cudaEventDestroy(join_ev);
   for (cudaEvent_t e : pending_ev) cudaEventDestroy(e);
   for (cudaEvent_t e : spare_ev) cudaEventDestroy(e);
   if (st) cudaStreamDestroy(st);

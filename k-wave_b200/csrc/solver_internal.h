@@ -91,6 +91,12 @@ class Session {
   int col_tl[3]{16, 16, 16};
   int rowL = 8;
   int slab = 1;  // z planes per chain slab
+  // slabs of a chain alternate between st and st2, forked and joined by
+  // events, so one slab's row kernel can run beside another's y passes
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  template <class F>
+  void for_slabs(F&& body);
   // captured steady-state step
   bool use_graph = true;
   cudaGraph_t graph = nullptr;

@@ -309,3 +309,26 @@ def test_config_2d_two_discs_cartesian_circle(interp):
     assert gpu["p"].shape == (50, kg.Nt)
     bad = {k: rel_l2(gpu[k], ora[k]) for k in ora if not rel_l2(gpu[k], ora[k]) <= TOL_LOSSLESS}
     assert not bad, bad
+
+
+def test_slabs_on_two_streams_give_identical_results():
+    """The y-inverse / row kernel / y-forward chains split into z slabs on two
+    streams (the default for large 3D grids) give bit-identical outputs."""
+    import os
+
+    from kwave import _lib
+
+    inp, record, start, _ = case_3d_het(n=(64, 48, 40), nt=30, record=("p", "p_max", "p_rms", "u", "p_final"))
+    whole = _lib.solve(inp, record, start_index=start)
+    old = {k: os.environ.get(k) for k in ("KWAVE_B200_SLAB", "KWAVE_B200_SLAB_STREAMS")}
+    os.environ.update(KWAVE_B200_SLAB="11", KWAVE_B200_SLAB_STREAMS="2")
+    try:
+        split = _lib.solve(inp, record, start_index=start)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    for k in whole:
+        np.testing.assert_array_equal(split[k], whole[k], err_msg=k)
