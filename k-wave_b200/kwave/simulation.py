@@ -61,21 +61,27 @@ def _find(mask):
     return np.flatnonzero(np.asarray(mask).reshape(-1, order="F")) + 1
 
 
-def _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0):
+def _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0, axisymmetric=False):
     """PMLInside = false: the grid grows by the PML on every side
     (kspaceFirstOrder_expandGridMatrices.m).  Medium maps extend their edge
     values, masks and p0 grow with zeros (p0 smoothed first, as
     kspaceFirstOrder_inputChecking.m:1499-1557 orders it), cuboid corners
     shift; Cartesian points keep their coordinates, which the centred grid
     preserves.  Returns the new grid, inputs and the slices that cut the
-    full-grid outputs back to the user's grid (kspaceFirstOrder3DC.m:586-614)."""
+    full-grid outputs back to the user's grid (kspaceFirstOrder3DC.m:586-614).
+    An axisymmetric grid grows radially at the outer radius only
+    (kspaceFirstOrder_expandGridMatrices.m:40-43, 65-66)."""
     import copy
 
     dim = kgrid.dim
-    pad = [(int(p), int(p)) for p in ps]
-    big = KWaveGrid(tuple(n + 2 * int(p) for n, p in zip(kgrid.N, ps)), kgrid.d)
+    lo = [int(p) for p in ps]
+    hi = [int(p) for p in ps]
+    if axisymmetric:
+        lo[1] = 0
+    pad = list(zip(lo, hi))
+    big = KWaveGrid(tuple(n + a + b for n, a, b in zip(kgrid.N, lo, hi)), kgrid.d)
     big.set_time(kgrid.Nt, kgrid.dt)
-    trim = tuple(slice(int(p), int(p) + n) for p, n in zip(ps, kgrid.N))
+    trim = tuple(slice(a, a + n) for a, n in zip(lo, kgrid.N))
 
     def grid_shaped(a):
         return np.ndim(a) == dim and tuple(np.shape(a)) == tuple(kgrid.N)
@@ -101,7 +107,9 @@ def _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0):
             p0 = np.asarray(source["p0"], dtype=np.float64)
             if p0.shape != tuple(kgrid.N):
                 raise ValueError("source.p0 must be the same size as the computational grid.")
-            source["p0"] = np.pad(smooth(p0, True) if smooth_p0 else p0, pad)
+            if smooth_p0:
+                p0 = smooth(_mirror_wswa(p0), True)[:, :p0.shape[1]] if axisymmetric else smooth(p0, True)
+            source["p0"] = np.pad(p0, pad)
         for k in ("p_mask", "u_mask"):
             if k in source:
                 source[k] = np.pad(np.asarray(source[k]), pad)
@@ -113,7 +121,7 @@ def _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0):
         if grid_shaped(mask) and not (mask.ndim == 2 and mask.shape[0] == 2 * dim and dim == 3):
             sensor["mask"] = np.pad(mask, pad)
         elif mask.ndim == 2 and mask.shape[0] == 2 * dim:
-            sh = np.asarray([int(p) for p in ps] * 2)[:, None]
+            sh = np.asarray(lo * 2)[:, None]
             sensor["mask"] = np.asarray(mask, dtype=np.int64) + sh
     return big, medium, source, sensor, trim
 
@@ -142,8 +150,6 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
     if axisymmetric:
         if kgrid.dim != 2:
             raise ValueError("axisymmetric simulations need a 2D grid")
-        if not pml_inside:
-            raise NotImplementedError("PMLInside = false is not supported for axisymmetric simulations")
         if isinstance(source, KWaveTransducer) or isinstance(sensor, KWaveTransducer):
             raise ValueError("Transducer inputs are only compatible with 3D simulations.")
         if "uy" in source:
@@ -156,7 +162,8 @@ def prepare(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, pml_s
     pa = np.broadcast_to(np.asarray(alpha_def if pml_alpha is None else pml_alpha, dtype=float), (dim,))
     trim = None
     if not pml_inside:
-        kgrid, medium, source, sensor, trim = _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0)
+        kgrid, medium, source, sensor, trim = _expand_grid(kgrid, medium, source, sensor, ps, smooth_p0,
+                                                           axisymmetric)
         smooth_p0 = False  # smoothed on the user's grid, before the expansion
     shape = kgrid.N
     # a transducer replaces the source struct, or serves as the sensor:

@@ -81,7 +81,8 @@ def test_input_file_matches_solve(tmp_path):
         np.testing.assert_array_equal(got[k], want[k], err_msg=k)
 
 
-def test_front_end():
+@pytest.mark.parametrize("inside", [True, False])
+def test_front_end(inside):
     from kwave import kspaceFirstOrderAS
     from kwave.simulation import postprocess, prepare
     from kwave.utils import KWaveGrid, make_disc
@@ -92,10 +93,14 @@ def test_front_end():
     p0 = 3 * make_disc(64, 32, 32, 1, 5)
     sensor = {"mask": np.pad(np.ones((1, 10)), ((40, 23), (0, 22))), "record": ["p", "p_max"]}
     medium = {"sound_speed": 1500.0, "density": 1000.0}
-    out = kspaceFirstOrderAS(kg, medium, {"p0": p0}, sensor, pml_size=8)
-    inp, record, start, meta = prepare(kg, medium, {"p0": p0}, sensor, pml_size=8, axisymmetric=True)
+    sensor["record"] = ["p", "p_max", "p_final"]
+    out = kspaceFirstOrderAS(kg, medium, {"p0": p0}, sensor, pml_size=8, pml_inside=inside)
+    inp, record, start, meta = prepare(kg, medium, {"p0": p0}, sensor, pml_size=8, axisymmetric=True,
+                                       pml_inside=inside)
     ora = postprocess(simulate_as(inp, record=record, dtype=np.float64), inp, meta)
-    assert rel_l2(out["p"], ora["p"]) <= TOL_LOSSLESS and rel_l2(out["p_max"], ora["p_max"]) <= TOL_LOSSLESS
+    assert out["p_final"].shape == (64, 32)
+    for k in ("p", "p_max", "p_final"):
+        assert rel_l2(out[k], ora[k]) <= TOL_LOSSLESS, k
 
 
 def test_rejects_what_it_does_not_run():

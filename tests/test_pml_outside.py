@@ -88,3 +88,19 @@ def test_outside_pml_agrees_with_free_space_before_the_wave_arrives():
     core = (slice(14, 50), slice(14, 50))
     err = np.linalg.norm(out[True][core] - out[False][core]) / np.linalg.norm(out[False][core])
     assert err < 2e-3, err
+
+
+def test_axisymmetric_grid_grows_at_the_outer_radius_only():
+    n, P = (40, 20), (6, 5)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    kg.set_time(20, 2e-8)
+    mask = np.zeros(n)
+    mask[10, 0] = mask[30, 7] = 1
+    inp, record, _, meta = prepare(kg, {"sound_speed": 1500.0}, {"p0": make_disc(*n, 20, 1, 4)},
+                                   {"mask": mask, "record": ["p", "p_final"]}, pml_size=P, pml_inside=False,
+                                   axisymmetric=True)
+    assert (inp["Nx"], inp["Ny"]) == (52, 25) and inp["axisymmetric_flag"] == 1
+    lin = np.flatnonzero(np.pad(mask, [(6, 6), (0, 5)]).reshape(-1, order="F")) + 1
+    np.testing.assert_array_equal(inp["sensor_mask_index"], lin)
+    out = postprocess({"p": np.zeros((2, 20), np.float32), "p_final": np.arange(52 * 25).reshape(52, 25)}, inp, meta)
+    assert out["p_final"].shape == n and out["p_final"][0, 0] == 6 * 25
