@@ -157,10 +157,6 @@ static bool factors_2357(uint64_t n) {
 // ---------------------------------------------------------------------------
 // Session
 // ---------------------------------------------------------------------------
-static std::vector<float> field_values(const kw_field& f) {
-  return std::vector<float>(f.data, f.data + f.numel);
-}
-
 template <class T>
 static T* up(DevBuf& b, const T* h, size_t n, cudaStream_t st) {
   b.alloc(n * sizeof(T), st);
@@ -332,6 +328,7 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     throw KwError(KW_ERR_INVALID_ARGUMENT, "Nx, Ny, Nz and Nt must be positive");
   p_rows0 = in->p_source_index_numel;
   u_rows0 = in->u_source_index_numel;
+  in_user = in;
   if (in->axisymmetric_flag) in = expand_axisymmetric(in);
   if (in->Ny == 1) throw KwError(KW_ERR_UNSUPPORTED, "1D simulations are not supported (Ny must be > 1)");
   for (uint64_t n : {in->Nx, in->Ny, in->Nz}) {
@@ -392,11 +389,13 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     }
     twd[a] = up(tw_buf[a], tw.data(), tw.size(), st);
   }
+  // runtime-engine tiles: the most lines (up to 16) whose shared-memory
+  // buffers stay under 160 KB; the schedule may lower them
   col_tl[0] = 16;
   for (int a = 1; a < d.dim; ++a) {
     int tl = 16;
     while (tl > 1 && (size_t)tl * ns[a] * 3 * 8 + ns[a] * 8 > 160 * 1024) tl /= 2;
-    col_tl[a] = tl;
+    col_tl[a] = col_tl_max[a] = tl;
   }
   rowL = std::max(1, std::min(8, 2048 / d.nx));
 
@@ -569,31 +568,6 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     if (use_tma[1] && !make_spec_map(&map_y[s], S_buf[s].p, d, 1, d.ny)) use_tma[1] = false;
     if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;
   }
-  // z slabs of the y-inverse / row kernel / y-forward chains.  Measured on
-  // 256^3: run one after another, slabs lose more to partial waves than L2
-  // reuse of a slab's half spectra gains (two slabs: 1.406 against 1.340 ms
-  // per step), but two slabs on two streams let one slab's latency-bound row
-  // kernel run beside the other's bandwidth-bound y passes (1.299 ms; four
-  // slabs 1.347).  So large 3D grids (2^22 points and more) take two slabs
-  // on two streams, others one slab.  KWAVE_B200_SLAB sets the planes per
-  // slab, KWAVE_B200_SLAB_STREAMS 1 or 2 the streams.
-  {
-    const bool big = d.dim == 3 && d.npts >= (1LL << 22) && d.nz >= 64;
-    int zs = big ? (d.nz + 1) / 2 : d.nz;
-    const char* env = std::getenv("KWAVE_B200_SLAB");
-    if (env && std::atoi(env) > 0) zs = std::min(std::atoi(env), d.nz);
-    const int nslab = (d.nz + zs - 1) / zs;
-    slab = (d.nz + nslab - 1) / nslab;
-    const char* two = std::getenv("KWAVE_B200_SLAB_STREAMS");
-    const int nst = (two && std::atoi(two) > 0) ? std::atoi(two) : (big ? 2 : 1);
-    if (nslab > 1 && nst >= 2) {
-      int lo = 0, hi = 0;
-      cudaDeviceGetStreamPriorityRange(&lo, &hi);
-      ck(cudaStreamCreateWithPriority(&st2, cudaStreamNonBlocking, lo), "cudaStreamCreate");
-      ck(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming), "cudaEventCreate");
-      ck(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming), "cudaEventCreate");
-    }
-  }
   if (eos == 1) ploc_buf.alloc(fb, st);
   if (opt.p_final) {
     p_buf.alloc(fb, st);
@@ -615,6 +589,10 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   // ----- sensors -----
   setup_sensors(in);
   timer.mark("sensors");
+  // ----- launch schedule: wisdom, tuning or the built-in choice -----
+  select_schedule();
+  in_user = nullptr;
+  timer.mark("schedule");
   ck(cudaStreamSynchronize(st), "setup");
 }
 
@@ -1786,6 +1764,17 @@ void* kw_session_stream(kw_session* s) { return s ? (void*)s->s->st : nullptr; }
 uint64_t kw_session_launches_per_step(const kw_session* s) { return s ? s->s->last_launches_per_step() : 0; }
 
 void kw_session_destroy(kw_session* s) { delete s; }
+
+int kw_session_schedule(const kw_session* s, kw_schedule* sched) {
+  if (!s || !sched) return KW_ERR_INVALID_ARGUMENT;
+  const kwb::Schedule c = s->s->schedule();
+  std::memset(sched, 0, sizeof(*sched));
+  sched->slab_planes = c.slab;
+  sched->streams = c.streams;
+  sched->row_lines = c.row_lines;
+  sched->col_lines = c.col_lines;
+  return KW_OK;
+}
 
 int kw_solve(const kw_input* in, const kw_options* opt, kw_output* out, kw_status* status) {
   return guarded(status, [&] {

@@ -19,6 +19,21 @@ struct KwError : std::runtime_error {
   KwError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// Launch shape of the time step, every choice of which gives bit-identical
+// results: the z slabs that the y-inverse / row kernel / y-forward chains
+// are split into and the streams the slabs alternate on, and the lines per
+// block of the runtime-plan engine's row and column kernels (compile-time
+// lengths have fixed tiles).
+struct Schedule {
+  int slab = 1;       // z planes per chain slab
+  int streams = 1;    // 1, or 2: slabs alternate between two streams
+  int row_lines = 8;  // runtime-engine row tiles (x)
+  int col_lines = 16; // runtime-engine column tiles (y and z)
+  bool operator==(const Schedule& o) const {
+    return slab == o.slab && streams == o.streams && row_lines == o.row_lines && col_lines == o.col_lines;
+  }
+};
+
 // Owning device allocation.
 struct DevBuf {
   void* p = nullptr;
@@ -52,6 +67,16 @@ class Session {
   void read(kw_output* out);
   uint64_t last_launches_per_step() const { return last_steps ? last_launches / last_steps : 0; }
   static size_t device_bytes_estimate(const kw_input* in, const kw_options* opt);
+  // launch schedule: the built-in choice for this grid, the one in use,
+  // the key it is tuned and cached under, and the candidates a tuner times
+  Schedule default_schedule() const;
+  Schedule schedule() const { return sched_; }
+  void set_schedule(const Schedule& s);  // waits for queued work; the step graph is captured again
+  std::string schedule_key() const;
+  std::vector<Schedule> schedule_candidates(int phase) const;
+  bool runtime_rows() const;
+  bool runtime_cols() const;
+  void select_schedule();  // end of setup(): wisdom, else tuning when enabled, else default_schedule()
 
   cudaStream_t st = nullptr;
   uint64_t Nt = 0;
@@ -89,8 +114,11 @@ class Session {
   FFTPlan plan[3]{};
   const float2* twd[3]{};
   int col_tl[3]{16, 16, 16};
+  int col_tl_max[3]{16, 16, 16};
   int rowL = 8;
   int slab = 1;  // z planes per chain slab
+  Schedule sched_{};
+  const kw_input* in_user = nullptr;  // the caller's input (before any axisymmetric expansion)
   // slabs of a chain alternate between st and st2, forked and joined by
   // events, so one slab's row kernel can run beside another's y passes
   cudaStream_t st2 = nullptr;
@@ -176,5 +204,16 @@ class Session {
   DevBuf p_raw_buf, p_max_buf, p_min_buf, p_rms_buf, p_rmsf_buf, p_maxall_buf, p_minall_buf;
   DevBuf u_raw_buf[3], u_max_buf[3], u_min_buf[3], u_rms_buf[3], u_rmsf_buf[3], u_maxall_buf[3], u_minall_buf[3];
 };
+
+// What tune_schedule() measured: the schedule chosen for the key, its device
+// time per step and the built-in default's, and how many schedules it timed
+// (0: the grid offers no choice).  The choice is remembered for the key.
+struct TuneOutcome {
+  std::string key;
+  Schedule chosen{};
+  float ms_chosen = 0.f, ms_default = 0.f;
+  int candidates = 0;
+};
+TuneOutcome tune_schedule(const kw_input* in, const kw_options* opt);
 
 }  // namespace kwb

@@ -90,6 +90,11 @@ class KwOutput(C.Structure):
     _fields_ = [(n, c_float_p) for n in OUTPUT_FIELDS]
 
 
+class KwSchedule(C.Structure):
+    _fields_ = [("slab_planes", C.c_int), ("streams", C.c_int), ("row_lines", C.c_int), ("col_lines", C.c_int),
+                ("candidates", C.c_int), ("ms_per_step", C.c_float), ("ms_default", C.c_float)]
+
+
 class KwOutputSizes(C.Structure):
     _fields_ = [("num_sensor_points", C.c_uint64), ("num_recorded_steps", C.c_uint64),
                 ("grid_points", C.c_uint64), ("device_bytes", C.c_uint64)]
@@ -101,6 +106,7 @@ EXPORTED = [
     "kw_session_steps_done", "kw_session_read", "kw_session_stream", "kw_session_launches_per_step",
     "kw_session_destroy", "kw_session_query", "kw_stream_priority_range", "kw_session_set_priority",
     "kw_session_save", "kw_session_restore",
+    "kw_tune", "kw_wisdom_import", "kw_wisdom_export", "kw_wisdom_forget", "kw_session_schedule",
     "kw_kspace_gradient_noalloc",
 ]
 
@@ -137,6 +143,12 @@ def _load():
     lib.kw_session_launches_per_step.argtypes = [C.c_void_p]
     lib.kw_session_launches_per_step.restype = C.c_uint64
     lib.kw_session_destroy.argtypes = [C.c_void_p]
+    lib.kw_tune.argtypes = [C.POINTER(KwInput), C.POINTER(KwOptions), C.POINTER(KwSchedule), C.POINTER(KwStatus)]
+    lib.kw_wisdom_import.argtypes = [C.c_char_p, C.POINTER(KwStatus)]
+    lib.kw_wisdom_export.argtypes = [C.c_char_p, C.POINTER(KwStatus)]
+    lib.kw_wisdom_forget.argtypes = []
+    lib.kw_wisdom_forget.restype = None
+    lib.kw_session_schedule.argtypes = [C.c_void_p, C.POINTER(KwSchedule)]
     lib.kw_kspace_gradient_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                                                C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p,
                                                C.POINTER(KwStatus)]
@@ -441,6 +453,15 @@ class Session:
     def launches_per_step(self):
         return int(lib.kw_session_launches_per_step(self._h))
 
+    @property
+    def schedule(self):
+        """The launch schedule the session runs with (kw_session_schedule)."""
+        sc = KwSchedule()
+        code = lib.kw_session_schedule(self._h, C.byref(sc))
+        if code != KW_OK:
+            raise KwaveError(code, "kw_session_schedule")
+        return _schedule_dict(sc)
+
     def read(self):
         out, bufs = alloc_outputs(self.inp, self.record, self.sizes)
         st = KwStatus()
@@ -454,6 +475,39 @@ class Session:
 
     def __del__(self):
         self.close()
+
+
+def _schedule_dict(sc):
+    return {"slab_planes": sc.slab_planes, "streams": sc.streams, "row_lines": sc.row_lines,
+            "col_lines": sc.col_lines, "candidates": sc.candidates, "ms_per_step": sc.ms_per_step,
+            "ms_default": sc.ms_default}
+
+
+def tune(inp: dict, record=("p",), start_index=1, device=-1):
+    """kw_tune(): time the launch schedules of this simulation's step on a
+    scratch copy and remember the fastest for its grid and step class.
+    Returns the chosen schedule with the measured ms per step."""
+    s, keep = make_input(inp)
+    opt = make_options(record, start_index, device)
+    sc = KwSchedule()
+    st = KwStatus()
+    _check(lib.kw_tune(C.byref(s), C.byref(opt), C.byref(sc), C.byref(st)), st)
+    del keep
+    return _schedule_dict(sc)
+
+
+def wisdom_import(path):
+    st = KwStatus()
+    _check(lib.kw_wisdom_import(os.fsencode(path), C.byref(st)), st)
+
+
+def wisdom_export(path):
+    st = KwStatus()
+    _check(lib.kw_wisdom_export(os.fsencode(path), C.byref(st)), st)
+
+
+def wisdom_forget():
+    lib.kw_wisdom_forget()
 
 
 def stream_priority_range():
