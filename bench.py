@@ -155,7 +155,7 @@ def traffic_per_step(n):
     return float(m.group(1)) * n ** 3
 
 
-def cpu_sample(inp, record, steps=3, warmup=2):
+def cpu_sample(inp, record, steps=5, warmup=2):
     """Time the oracle (numpy/scipy, all host threads) on the first
     warmup+steps time steps of the same workload."""
     from oracle.kspace_oracle import simulate
@@ -165,7 +165,7 @@ def cpu_sample(inp, record, steps=3, warmup=2):
              on_step=lambda t: stamps.append(time.perf_counter()))
     per = (stamps[-1] - stamps[warmup - 1]) / steps
     npts = int(inp["Nx"]) * int(inp["Ny"]) * int(inp["Nz"])
-    return npts / per, per
+    return npts / per, per, warmup, steps
 
 
 def replica_throughput(ms_local, units_local, dist=None, device=None):
@@ -480,10 +480,11 @@ def main():
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, per = cpu_sample(inp, record)
+        v, per, w, k = cpu_sample(inp, record)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                "sample": f"time steps 3..5 of the same {args.n}^3 run, oracle (numpy/scipy.fft, "
-                                          f"all host threads), {per:.2f} s/step"}
+                                "sample": f"time steps {w + 1}..{w + k} of the same {args.n}^3 run, oracle "
+                                          f"(numpy/scipy.fft, all host threads), {per:.2f} s/step, "
+                                          f"{per * k:.1f} s timed"}
     if rank == 0 and world == 1 and not args.shape:
         if args.batch_sims > 0:
             line["batched"] = batched_sample(args.batch_sims, args.batch_nt)

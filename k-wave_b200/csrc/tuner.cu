@@ -16,6 +16,7 @@
 // Radix plans are not tuned: a different factorisation rounds differently,
 // and results must not depend on timing noise.
 #include <cuda_runtime.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -93,7 +94,7 @@ void export_file(const std::string& path) {
     if (f) parse_wisdom(f, all);
   }
   for (auto& kv : g_wisdom) all[kv.first] = kv.second;
-  const std::string tmp = path + ".tmp";
+  const std::string tmp = path + ".tmp." + std::to_string((long)getpid());  // one per writing process
   {
     std::ofstream o(tmp);
     if (!o) throw KwError(KW_ERR_IO, "cannot write wisdom file " + tmp);
@@ -321,7 +322,13 @@ void Session::select_schedule() {
       size_t free_b = 0, total_b = 0;
       cuda_ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
       const size_t need = device_bytes_estimate(in_user, &opt) * 5 / 4 + (256u << 20);
-      if (free_b > need) s = tune_schedule(in_user, &opt).chosen;
+      if (free_b > need) {
+        try {
+          s = tune_schedule(in_user, &opt).chosen;
+        } catch (const KwError& e) {
+          if (e.code != KW_ERR_OUT_OF_MEMORY) throw;  // no room after all: the built-in schedule
+        }
+      }
     }
   }
   set_schedule(s);
