@@ -280,17 +280,20 @@ void kw_session_destroy(kw_session* s);
 /*
  * No counterpart in the reference (its binaries launch one fixed way).
  *
- * Launch schedule of the time step.  Every schedule gives bit-identical
- * results; they differ in speed: the y-inverse / row / y-forward chains of a
- * 3D step run whole or as z slabs, the slabs on one stream or alternating
- * between two, and the runtime-plan FFT kernels (lengths with a factor 7, or
- * outside 64..1024) transform a chosen number of lines per block.
+ * Launch schedule of the time step.  The y-inverse / row / y-forward chains
+ * of a 3D step run whole or as z slabs, the slabs on one stream or
+ * alternating between two, and the runtime-plan FFT kernels (lengths with a
+ * factor 7, or outside 64..1024) transform a chosen number of lines per
+ * block: these give bit-identical results.  The runtime-plan engine's radix
+ * order can be chosen too (0: radix 16 first, 1: odd radices first, 2: no
+ * radix 16); another order rounds differently, within FP32 rounding.
  */
 typedef struct {
   int slab_planes;   /* z planes per slab (Nz: the chains are not split) */
   int streams;       /* 1, or 2: slabs alternate between two streams */
   int row_lines;     /* lines per block of runtime-plan row (x) kernels */
   int col_lines;     /* cap on lines per block of runtime-plan column kernels */
+  int radix_plan;    /* radix order of the runtime-plan engine (0, 1, 2) */
   int candidates;    /* schedules kw_tune timed (0: the grid offers no choice) */
   float ms_per_step; /* device time per step of the chosen schedule */
   float ms_default;  /* device time per step of the built-in schedule */
@@ -302,15 +305,15 @@ typedef struct {
  * the copy needs about the device memory of kw_output_sizes' device_bytes)
  * and remember the fastest for this grid, step class and device: sessions
  * and solves created afterwards in the process use it.  A challenger must
- * beat the built-in schedule by more than 1 %.  Takes about 80 time steps
- * plus one set-up.  With KWAVE_B200_WISDOM=<file> the remembered schedules
+ * beat the current choice by more than 1 %.  Takes up to about 200 time
+ * steps (80 on compile-time lengths) plus one set-up.  With KWAVE_B200_WISDOM=<file> the remembered schedules
  * are merged into that file and read from it by the first session of a
  * process; with KWAVE_B200_TUNE=1 a session whose key is not remembered
  * tunes itself at creation when free device memory allows.
  */
 int kw_tune(const kw_input* in, const kw_options* opt, kw_schedule* chosen, kw_status* status);
 /* Read / write remembered schedules (text: key slab_planes streams row_lines
- * col_lines ms_per_step).  Export merges into an existing file. */
+ * col_lines radix_plan ms_per_step).  Export merges into an existing file. */
 int kw_wisdom_import(const char* path, kw_status* status);
 int kw_wisdom_export(const char* path, kw_status* status);
 /* Forget every remembered schedule (and do not read KWAVE_B200_WISDOM again). */

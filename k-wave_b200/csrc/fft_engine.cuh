@@ -271,20 +271,25 @@ __device__ float2* fft_lines(float2* a, float2* b, const float2* __restrict__ tw
   return a;
 }
 
-// Host-side plan construction: radix-16 stages first, then 8/4/2, then 7, 5, 3.
+// Host-side plan construction.  Radix orders (variant):
+//   0: radix-16 stages first, then 8 / 4 / 2, then 7, 5, 3 (fewest stages);
+//   1: the odd radices 7, 5, 3 first, then 16, 8, 4, 2;
+//   2: no radix-16 stage (8 / 4 / 2, then 7, 5, 3): more stages, lighter
+//      butterflies.
+// Every order computes the same transform; they round differently.
 // Returns false when n has a prime factor other than 2, 3, 5 or 7.
-inline bool make_fft_plan(int n, FFTPlan* p) {
+inline bool make_fft_plan(int n, FFTPlan* p, int variant = 0) {
   p->n = n;
   p->nst = 0;
   int m = n;
-  if (n < 1) return false;
-  while (m % 16 == 0) { p->rad[p->nst++] = 16; m /= 16; }
-  const int rs[6] = {8, 4, 2, 7, 5, 3};
-  for (int i = 0; i < 6; ++i) {
-    while (m % rs[i] == 0) {
+  if (n < 1 || variant < 0 || variant > 2) return false;
+  const int order[3][7] = {{16, 8, 4, 2, 7, 5, 3}, {7, 5, 3, 16, 8, 4, 2}, {8, 4, 2, 7, 5, 3, 0}};
+  for (int i = 0; i < 7 && order[variant][i]; ++i) {
+    const int r = order[variant][i];
+    while (m % r == 0) {
       if (p->nst >= KWB_MAX_STAGES) return false;
-      p->rad[p->nst++] = rs[i];
-      m /= rs[i];
+      p->rad[p->nst++] = r;
+      m /= r;
     }
   }
   return m == 1;

@@ -1773,6 +1773,7 @@ int kw_session_schedule(const kw_session* s, kw_schedule* sched) {
   sched->streams = c.streams;
   sched->row_lines = c.row_lines;
   sched->col_lines = c.col_lines;
+  sched->radix_plan = c.radix;
   return KW_OK;
 }
 

@@ -19,18 +19,21 @@ struct KwError : std::runtime_error {
   KwError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
-// Launch shape of the time step, every choice of which gives bit-identical
-// results: the z slabs that the y-inverse / row kernel / y-forward chains
-// are split into and the streams the slabs alternate on, and the lines per
-// block of the runtime-plan engine's row and column kernels (compile-time
-// lengths have fixed tiles).
+// Launch shape of the time step: the z slabs that the y-inverse / row
+// kernel / y-forward chains are split into and the streams the slabs
+// alternate on, and the lines per block of the runtime-plan engine's row and
+// column kernels (compile-time lengths have fixed tiles) -- choices that give
+// bit-identical results -- and the radix order of the runtime-plan engine
+// (make_fft_plan variant), which rounds differently.
 struct Schedule {
   int slab = 1;       // z planes per chain slab
   int streams = 1;    // 1, or 2: slabs alternate between two streams
   int row_lines = 8;  // runtime-engine row tiles (x)
   int col_lines = 16; // runtime-engine column tiles (y and z)
+  int radix = 0;      // runtime-engine radix order
   bool operator==(const Schedule& o) const {
-    return slab == o.slab && streams == o.streams && row_lines == o.row_lines && col_lines == o.col_lines;
+    return slab == o.slab && streams == o.streams && row_lines == o.row_lines && col_lines == o.col_lines &&
+           radix == o.radix;
   }
 };
 

@@ -5,7 +5,10 @@
 // z slabs, the slabs one after another on one stream or alternating between
 // two (one slab's latency-bound row kernel then runs beside the other's
 // bandwidth-bound y passes), and, for lengths served by the runtime-plan FFT
-// engine, the number of lines each row or column block transforms.  Which is
+// engine, the number of lines each row or column block transforms.  That
+// engine's radix order can be chosen too; another order rounds differently
+// (FP32 rounding, far inside the solver's tolerance), and once chosen it is
+// kept for the key, so the runs of a process agree bit for bit.  Which is
 // fastest depends on the grid and on the step's kernels, so the tuner times
 // the candidates on a scratch copy of the simulation (same grid, medium,
 // sources, sensor reductions; no recorded series) and keeps the fastest in a
@@ -13,8 +16,6 @@
 // plans as wisdom.  Sessions created later for the same key use it; the
 // table can be written to and read from a text file (KWAVE_B200_WISDOM), so
 // a binary started once per simulation reuses what an earlier run measured.
-// Radix plans are not tuned: a different factorisation rounds differently,
-// and results must not depend on timing noise.
 #include <cuda_runtime.h>
 #include <unistd.h>
 
@@ -52,20 +53,47 @@ int env_int(const char* name) {
   return v ? std::atoi(v) : 0;
 }
 
-// Parse wisdom lines "<key> <slab> <streams> <row_lines> <col_lines> <ms>"
-// into `into`; '#' lines are comments.  Returns the entries read.
+// Parse wisdom lines "<key> <slab> <streams> <row_lines> <col_lines> <radix>
+// <ms>" into `into`; '#' lines are comments.  Returns the entries read.
 int parse_wisdom(std::istream& is, std::map<std::string, std::pair<Schedule, float>>& into) {
   std::string line;
   int n = 0;
   while (std::getline(is, line)) {
     if (line.empty() || line[0] == '#') continue;
     std::istringstream ls(line);
-    std::string key;
+    std::vector<std::string> tok;
+    for (std::string t; ls >> t;) tok.push_back(t);
+    if (tok.empty()) continue;
     Schedule s;
     float ms = 0.f;
-    if (!(ls >> key >> s.slab >> s.streams >> s.row_lines >> s.col_lines >> ms))
+    // whole-token integers and a number: "1.0" is not a schedule field
+    auto to_int = [&](const std::string& t) {
+      size_t used = 0;
+      int v = 0;
+      try {
+        v = std::stoi(t, &used);
+      } catch (const std::exception&) {
+        used = 0;
+      }
+      if (used != t.size() || t.empty()) throw KwError(KW_ERR_IO, "malformed wisdom line: " + line);
+      return v;
+    };
+    if (tok.size() != 7) throw KwError(KW_ERR_IO, "malformed wisdom line: " + line);
+    const std::string key = tok[0];
+    s.slab = to_int(tok[1]);
+    s.streams = to_int(tok[2]);
+    s.row_lines = to_int(tok[3]);
+    s.col_lines = to_int(tok[4]);
+    s.radix = to_int(tok[5]);
+    try {
+      size_t used = 0;
+      ms = std::stof(tok[6], &used);
+      if (used != tok[6].size()) throw std::invalid_argument("trailing");
+    } catch (const std::exception&) {
       throw KwError(KW_ERR_IO, "malformed wisdom line: " + line);
-    if (s.slab < 1 || s.streams < 1 || s.streams > 2 || s.row_lines < 1 || s.col_lines < 1)
+    }
+    if (s.slab < 1 || s.streams < 1 || s.streams > 2 || s.row_lines < 1 || s.col_lines < 1 || s.radix < 0 ||
+        s.radix > 2)
       throw KwError(KW_ERR_IO, "wisdom entry out of range: " + line);
     into[key] = {s, ms};
     ++n;
@@ -98,11 +126,11 @@ void export_file(const std::string& path) {
   {
     std::ofstream o(tmp);
     if (!o) throw KwError(KW_ERR_IO, "cannot write wisdom file " + tmp);
-    o << "# kwave_b200 launch-schedule wisdom: key slab_planes streams row_lines col_lines ms_per_step\n";
+    o << "# kwave_b200 launch-schedule wisdom: key slab_planes streams row_lines col_lines radix_plan ms_per_step\n";
     for (auto& kv : all) {
       const Schedule& s = kv.second.first;
       o << kv.first << ' ' << s.slab << ' ' << s.streams << ' ' << s.row_lines << ' ' << s.col_lines << ' '
-        << kv.second.second << '\n';
+        << s.radix << ' ' << kv.second.second << '\n';
     }
     if (!o) throw KwError(KW_ERR_IO, "cannot write wisdom file " + tmp);
   }
@@ -141,6 +169,7 @@ Schedule normalise(Schedule s, const Dims& d, int row_max) {
   s.streams = (nslab > 1 && s.streams >= 2) ? 2 : 1;
   s.row_lines = std::max(1, std::min(s.row_lines, row_max));
   s.col_lines = std::max(1, std::min(s.col_lines, 16));
+  s.radix = std::max(0, std::min(s.radix, 2));
   return s;
 }
 
@@ -197,6 +226,10 @@ void Session::set_schedule(const Schedule& s0) {
   slab = s.slab;
   rowL = s.row_lines;
   for (int a = 1; a < d.dim; ++a) col_tl[a] = std::min(col_tl_max[a], s.col_lines);
+  const int ns[3] = {d.nx, d.ny, d.nz};
+  for (int a = 0; a < d.dim; ++a)
+    if (!ct_supported(ns[a]) && !make_fft_plan(ns[a], &plan[a], s.radix))
+      throw KwError(KW_ERR_INTERNAL, "no radix plan of this order for " + std::to_string(ns[a]));
   sched_ = s;
 }
 
@@ -215,7 +248,8 @@ std::string Session::schedule_key() const {
 }
 
 // Phase 0: slab splits and streams (3D grids of 16 planes or more), the
-// current schedule first.  Phase 1: halved runtime-engine tiles.
+// current schedule first.  Phase 1: halved runtime-engine tiles.  Phase 2:
+// the runtime engine's other radix orders, where they give other plans.
 std::vector<Schedule> Session::schedule_candidates(int phase) const {
   std::vector<Schedule> c{sched_};
   auto add = [&](Schedule s) {
@@ -232,7 +266,7 @@ std::vector<Schedule> Session::schedule_candidates(int phase) const {
         add(s);
       }
     }
-  } else {
+  } else if (phase == 1) {
     if (runtime_rows() && sched_.row_lines > 1) {
       Schedule s = sched_;
       s.row_lines = sched_.row_lines / 2;
@@ -248,13 +282,30 @@ std::vector<Schedule> Session::schedule_candidates(int phase) const {
         add(s);
       }
     }
+  } else if (phase == 2) {
+    const int ns[3] = {d.nx, d.ny, d.nz};
+    for (int v = 0; v <= 2; ++v) {
+      if (v == sched_.radix) continue;
+      bool differs = false;
+      for (int a = 0; a < d.dim; ++a) {
+        if (ct_supported(ns[a])) continue;
+        FFTPlan p0{}, p1{};
+        if (!make_fft_plan(ns[a], &p0, sched_.radix) || !make_fft_plan(ns[a], &p1, v)) continue;
+        differs = differs || p0.nst != p1.nst || !std::equal(p0.rad, p0.rad + p0.nst, p1.rad);
+      }
+      if (differs) {
+        Schedule s = sched_;
+        s.radix = v;
+        add(s);
+      }
+    }
   }
   return c;
 }
 
 TuneOutcome tune_schedule(const kw_input* in, const kw_options* opt) {
   if (!in || !opt) throw KwError(KW_ERR_INVALID_ARGUMENT, "input and options must not be NULL");
-  constexpr int kTimed = 6, kWarm = 2, kRounds = 2, kMaxCand = 9;
+  constexpr int kTimed = 6, kWarm = 2, kRounds = 2, kMaxCand = 12;
   kw_input in2 = *in;
   kw_options o2 = *opt;
   // recorded series are left out (their memory grows with Nt); reductions stay
@@ -287,7 +338,7 @@ TuneOutcome tune_schedule(const kw_input* in, const kw_options* opt) {
     tmp.sync();
     return best;
   };
-  for (int phase = 0; phase < 2; ++phase) {
+  for (int phase = 0; phase < 3; ++phase) {
     tmp.set_schedule(r.chosen);
     const std::vector<Schedule> cands = tmp.schedule_candidates(phase);
     if (cands.size() < 2) continue;
@@ -368,6 +419,7 @@ void fill(kw_schedule* out, const kwb::Schedule& s) {
   out->streams = s.streams;
   out->row_lines = s.row_lines;
   out->col_lines = s.col_lines;
+  out->radix_plan = s.radix;
 }
 
 }  // namespace

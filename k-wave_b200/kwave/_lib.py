@@ -92,7 +92,8 @@ class KwOutput(C.Structure):
 
 class KwSchedule(C.Structure):
     _fields_ = [("slab_planes", C.c_int), ("streams", C.c_int), ("row_lines", C.c_int), ("col_lines", C.c_int),
-                ("candidates", C.c_int), ("ms_per_step", C.c_float), ("ms_default", C.c_float)]
+                ("radix_plan", C.c_int), ("candidates", C.c_int), ("ms_per_step", C.c_float),
+                ("ms_default", C.c_float)]
 
 
 class KwOutputSizes(C.Structure):
@@ -479,8 +480,8 @@ class Session:
 
 def _schedule_dict(sc):
     return {"slab_planes": sc.slab_planes, "streams": sc.streams, "row_lines": sc.row_lines,
-            "col_lines": sc.col_lines, "candidates": sc.candidates, "ms_per_step": sc.ms_per_step,
-            "ms_default": sc.ms_default}
+            "col_lines": sc.col_lines, "radix_plan": sc.radix_plan, "candidates": sc.candidates,
+            "ms_per_step": sc.ms_per_step, "ms_default": sc.ms_default}
 
 
 def tune(inp: dict, record=("p",), start_index=1, device=-1):

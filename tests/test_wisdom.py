@@ -11,26 +11,28 @@ def _entries(path):
 
 def test_import_export_round_trip_and_merge(tmp_path):
     a = tmp_path / "a.txt"
-    a.write_text("# comment\n256x256x256/eos1/nl1/as0/dense1/sm10.0148 128 2 8 16 1.299\n"
-                 "100x120x90/eos1/nl0/as0/dense0/sm10.0148 90 1 4 8 0.48\n")
+    a.write_text("# comment\n256x256x256/eos1/nl1/as0/dense1/sm10.0148 128 2 8 16 0 1.299\n"
+                 "100x120x90/eos1/nl0/as0/dense0/sm10.0148 90 1 4 8 2 0.48\n")
     _lib.wisdom_forget()
     _lib.wisdom_import(str(a))
     out = tmp_path / "out.txt"
-    out.write_text("64x48x40/eos1/nl1/as0/dense0/sm10.0148 20 2 8 16 0.05\n")
+    out.write_text("64x48x40/eos1/nl1/as0/dense0/sm10.0148 20 2 8 16 1 0.05\n")
     _lib.wisdom_export(str(out))  # merges: the file's entry stays, the table's are added
     got = _entries(out)
     assert [e[0] for e in got] == sorted(["256x256x256/eos1/nl1/as0/dense1/sm10.0148",
                                           "100x120x90/eos1/nl0/as0/dense0/sm10.0148",
                                           "64x48x40/eos1/nl1/as0/dense0/sm10.0148"])
     row = dict((e[0], e[1:]) for e in got)["256x256x256/eos1/nl1/as0/dense1/sm10.0148"]
-    assert row[:4] == ["128", "2", "8", "16"] and abs(float(row[4]) - 1.299) < 1e-6
+    assert row[:5] == ["128", "2", "8", "16", "0"] and abs(float(row[5]) - 1.299) < 1e-6
+    assert dict((e[0], e[1:]) for e in got)["100x120x90/eos1/nl0/as0/dense0/sm10.0148"][4] == "2"
     _lib.wisdom_forget()
     empty = tmp_path / "empty.txt"
     _lib.wisdom_export(str(empty))
     assert _entries(empty) == []
 
 
-@pytest.mark.parametrize("text", ["key 1 2 3\n", "key 0 1 8 16 1.0\n", "key 4 3 8 16 1.0\n", "key a b c d e\n"])
+@pytest.mark.parametrize("text", ["key 1 2 3\n", "key 0 1 8 16 0 1.0\n", "key 4 3 8 16 0 1.0\n",
+                                  "key 4 2 8 16 3 1.0\n", "key 4 2 8 16 1.0\n", "key a b c d e f\n"])
 def test_malformed_wisdom_is_rejected(tmp_path, text):
     p = tmp_path / "bad.txt"
     p.write_text(text)
