@@ -185,6 +185,12 @@ def replica_throughput(ms_local, units_local, dist=None, device=None):
     return units_all / (ms_max / 1e3), ms_max
 
 
+def _lib_batch(sessions):
+    from kwave import _lib
+
+    return _lib.Batch(sessions)
+
+
 def batched_sample(n_sims, nt, chunk=25):
     """Config of many independent 3D linear lossy simulations on uneven
     2^a 3^b 5^c grids (64..192 per edge): grid-point-steps/s when they advance
@@ -232,7 +238,7 @@ def batched_sample(n_sims, nt, chunk=25):
     work_s = sum(int(inputs[i]["Nx"]) * int(inputs[i]["Ny"]) * int(inputs[i]["Nz"]) * int(inputs[i]["Nt"])
                  for i in sample)
     res["plain_dropin"] = work_s / (time.perf_counter() - t0)
-    for mode in ("plain", "batched"):
+    for mode in ("plain", "batched", "batched_graph"):
         sessions = [serving.gpu_session(inp, record) for inp in inputs]
         for s_ in sessions:
             s_.sync()
@@ -242,6 +248,13 @@ def batched_sample(n_sims, nt, chunk=25):
             for s_, inp in zip(sessions, inputs):
                 s_.advance(int(inp["Nt"]))
                 s_.sync()
+        elif mode == "batched_graph":  # one kw_batch: each step of all 48 one graph launch
+            b = _lib_batch(sessions)
+            for _ in range(0, max(int(i["Nt"]) for i in inputs), chunk):
+                b.advance(chunk)
+            b.sync()
+            res["graph_launches"] = b.graph_launches
+            b.close()
         else:
             left = [int(i["Nt"]) for i in inputs]
             while any(left):
@@ -254,15 +267,22 @@ def batched_sample(n_sims, nt, chunk=25):
                 s_.sync()
         torch.cuda.synchronize()
         res[mode] = work / (time.perf_counter() - t0)
+        if mode == "batched_graph":
+            same = same and all(all(np.array_equal(r[k], o[k]) for k in o)
+                                for r, o in zip((s_.read() for s_ in sessions), outs))
         for s_ in sessions:
             s_.close()
     return {"workload": f"{n_sims} independent 3D linear lossy sims, edges 64..192 (5-smooth), y 1.1, "
                         f"200 sensor points, Nt {nt}, FP32", "unit": UNIT,
             "batched": res["batched"], "plain": res["plain"], "speedup": res["batched"] / res["plain"],
+            "batched_graph": res["batched_graph"], "graph_speedup": res["batched_graph"] / res["plain"],
+            "graph_launches": res["graph_launches"],
             "batched_e2e": res["batched_e2e"], "plain_dropin": res["plain_dropin"],
             "speedup_vs_dropin": res["batched_e2e"] / res["plain_dropin"], "results_identical": same,
             "timing": "host clock around a device synchronize.  batched / plain: resident sessions created "
-                      "before the timed region, advanced together / one at a time.  batched_e2e: run_batch "
+                      "before the timed region, advanced together (each on its own stream) / one at a time.  "
+                      "batched_graph: the same sessions in one kw_batch, each time step of all of them one "
+                      "CUDA graph launch.  batched_e2e: run_batch "
                       "including set-up, uploads and read-back.  plain_dropin: every third simulation, each "
                       "with its input file written, the solver binary run and the output file read, one at a "
                       "time (grid-point-steps of those simulations / their wall time)"}

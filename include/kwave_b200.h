@@ -278,6 +278,30 @@ uint64_t kw_session_launches_per_step(const kw_session* s);
 void kw_session_destroy(kw_session* s);
 
 /*
+ * No counterpart in the reference (one solve per process there).
+ *
+ * Batches: many resident sessions advanced together, each time step of all
+ * of them one CUDA graph launch (a parent graph whose independent branches
+ * are the sessions' captured steps, so their kernels run side by side).
+ * Steps that cannot be replayed (an initial-pressure start, a session's
+ * last step, steps of a per-point corrected source) run on their own, in
+ * order.  Sessions with different Nt stop at their own last step.  Work is
+ * enqueued after each member's queued work, and each member's later work
+ * (kw_session_read, kw_session_sync) waits for it.  Streamed sessions
+ * cannot be batched.  Results are bit for bit those of kw_session_advance.
+ */
+typedef struct kw_batch kw_batch;
+int kw_batch_create(kw_session* const* sessions, int n, kw_batch** batch, kw_status* status);
+int kw_batch_advance(kw_batch* b, uint64_t nsteps, kw_status* status);
+/* Device time of the last kw_batch_advance() in ms (synchronises). */
+int kw_batch_elapsed_ms(kw_batch* b, float* ms, kw_status* status);
+int kw_batch_sync(kw_batch* b, kw_status* status);
+/* Parent-graph launches so far: one per time step advanced as a batch. */
+uint64_t kw_batch_graph_launches(const kw_batch* b);
+/* Destroys the batch only (its sessions stay). */
+void kw_batch_destroy(kw_batch* b);
+
+/*
  * No counterpart in the reference (its binaries launch one fixed way).
  *
  * Launch schedule of the time step.  The y-inverse / row / y-forward chains

@@ -1224,6 +1224,7 @@ void Session::enqueue_step() {
       launches_ = l0;
       ck(cudaStreamEndCapture(st, &g), "end capture");
       graph = g;
+      ++graph_gen;
       ck(cudaGraphInstantiate(&graph_exec, graph, 0), "graph instantiate");
     }
     ck(cudaGraphLaunch(graph_exec, st), "graph launch");
@@ -1608,10 +1609,6 @@ size_t Session::device_bytes_estimate(const kw_input* in, const kw_options* o) {
 // ---------------------------------------------------------------------------
 using kwb::KwError;
 using kwb::Session;
-
-struct kw_session {
-  std::unique_ptr<Session> s;
-};
 
 static int set_status(kw_status* st, int code, const std::string& msg) {
   if (st) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <deque>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -48,7 +49,11 @@ struct DevBuf {
   void alloc(size_t nbytes, cudaStream_t st);
 };
 
+class Batch;
+
 class Session {
+  friend class Batch;  // advances member sessions' captured steps as one graph
+
  public:
   ~Session();
   // allow_ring: the caller drains raw series in blocks (drain_raw), so they
@@ -133,6 +138,7 @@ class Session {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   uint64_t graph_launches = 0;
+  uint64_t graph_gen = 0;  // captures so far (a batch rebuilds its parent graph when this changes)
   SpecTables T{};
   float dtf = 0.f;
   bool nonlinear = false;
@@ -220,3 +226,8 @@ struct TuneOutcome {
 TuneOutcome tune_schedule(const kw_input* in, const kw_options* opt);
 
 }  // namespace kwb
+
+// The C ABI's session handle.
+struct kw_session {
+  std::unique_ptr<kwb::Session> s;
+};

@@ -108,6 +108,8 @@ EXPORTED = [
     "kw_session_destroy", "kw_session_query", "kw_stream_priority_range", "kw_session_set_priority",
     "kw_session_save", "kw_session_restore",
     "kw_tune", "kw_wisdom_import", "kw_wisdom_export", "kw_wisdom_forget", "kw_session_schedule",
+    "kw_batch_create", "kw_batch_advance", "kw_batch_elapsed_ms", "kw_batch_sync", "kw_batch_graph_launches",
+    "kw_batch_destroy",
     "kw_kspace_gradient_noalloc",
 ]
 
@@ -150,6 +152,13 @@ def _load():
     lib.kw_wisdom_forget.argtypes = []
     lib.kw_wisdom_forget.restype = None
     lib.kw_session_schedule.argtypes = [C.c_void_p, C.POINTER(KwSchedule)]
+    lib.kw_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p), C.POINTER(KwStatus)]
+    lib.kw_batch_advance.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(KwStatus)]
+    lib.kw_batch_elapsed_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(KwStatus)]
+    lib.kw_batch_sync.argtypes = [C.c_void_p, C.POINTER(KwStatus)]
+    lib.kw_batch_graph_launches.argtypes = [C.c_void_p]
+    lib.kw_batch_graph_launches.restype = C.c_uint64
+    lib.kw_batch_destroy.argtypes = [C.c_void_p]
     lib.kw_kspace_gradient_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                                                C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p,
                                                C.POINTER(KwStatus)]
@@ -472,6 +481,45 @@ class Session:
     def close(self):
         if getattr(self, "_h", None):
             lib.kw_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Sessions advanced together, one CUDA graph launch per time step for
+    all of them (kw_batch_*).  The sessions stay owned by the caller."""
+
+    def __init__(self, sessions):
+        self.sessions = list(sessions)
+        arr = (C.c_void_p * len(self.sessions))(*[s._h.value for s in self.sessions])
+        h = C.c_void_p()
+        st = KwStatus()
+        _check(lib.kw_batch_create(arr, len(self.sessions), C.byref(h), C.byref(st)), st)
+        self._h = h
+
+    def advance(self, n):
+        st = KwStatus()
+        _check(lib.kw_batch_advance(self._h, C.c_uint64(int(n)), C.byref(st)), st)
+
+    def elapsed_ms(self):
+        st = KwStatus()
+        ms = C.c_float()
+        _check(lib.kw_batch_elapsed_ms(self._h, C.byref(ms), C.byref(st)), st)
+        return ms.value
+
+    def sync(self):
+        st = KwStatus()
+        _check(lib.kw_batch_sync(self._h, C.byref(st)), st)
+
+    @property
+    def graph_launches(self):
+        return int(lib.kw_batch_graph_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.kw_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -127,21 +127,36 @@ class Request:
         return int(self.inp["Nx"]) * int(self.inp["Ny"]) * int(self.inp["Nz"]) * int(self.inp["Nt"])
 
 
-def run_batch(inputs, record=("p",), chunk=25, factory=gpu_session, sync=True):
-    """Advance every simulation in `inputs` to its last step, interleaving
-    them in chunks of `chunk` steps, and return their outputs in order.
+def run_batch(inputs, record=("p",), chunk=25, factory=gpu_session, sync=True, mode="streams"):
+    """Advance every simulation in `inputs` to its last step and return their
+    outputs in order.
 
-    Work is only enqueued here (each session's steps go to its own stream),
-    so the device runs the simulations concurrently."""
+    mode "streams": the sessions are interleaved in chunks of `chunk` steps,
+    each session's steps on its own stream, so the device runs them
+    concurrently.  mode "graph": one kw_batch advances them all, each time
+    step of every simulation one CUDA graph launch (library sessions only).
+    Work is only enqueued until the outputs are read."""
     sessions = [factory(inp, record) for inp in inputs]
     try:
-        left = [int(inp["Nt"]) for inp in inputs]
-        while any(left):
-            for i, s in enumerate(sessions):
-                if left[i]:
-                    n = min(chunk, left[i])
-                    s.advance(n)
-                    left[i] -= n
+        if mode == "graph":
+            from ._lib import Batch
+
+            b = Batch(sessions)
+            try:
+                for _ in range(0, max(int(inp["Nt"]) for inp in inputs), chunk):
+                    b.advance(chunk)
+            finally:
+                b.close()
+        elif mode == "streams":
+            left = [int(inp["Nt"]) for inp in inputs]
+            while any(left):
+                for i, s in enumerate(sessions):
+                    if left[i]:
+                        n = min(chunk, left[i])
+                        s.advance(n)
+                        left[i] -= n
+        else:
+            raise ValueError(f"unknown batch mode {mode!r}")
         return [s.read() for s in sessions] if sync else sessions
     finally:
         if sync:
