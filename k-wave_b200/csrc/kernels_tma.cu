@@ -1,5 +1,7 @@
 // Persistent, TMA-fed column passes (the y pass and the fused last-axis
-// operator) for compile-time transform lengths up to 256.
+// operator) for compile-time transform lengths up to 256 (the y pass: every
+// 2^a 3^b 5^c length from 64 to 256; the fused operator: the two-stage
+// lengths 64, 128, 256, whose register hand-off it is built on).
 //
 // Each thread block loops over column tiles (TL adjacent kx columns x the
 // whole line).  Tiles arrive by cp.async.bulk.tensor into a ring of shared
@@ -20,10 +22,17 @@
 
 namespace kwb {
 
+// Lines per TMA tile: the compile-time tile's line count rounded down to an
+// even number, so every tile starts at a bin index x = cx * LINES whose byte
+// offset (8-byte bins) is a multiple of 16, as tensor copies require.
+__host__ __device__ constexpr int tma_lines_of(int n) {
+  return ct_lines_of(n) & ~1;  // ct_lines_of is at least 4
+}
+
 template <int NC>
 struct TTile {
-  static constexpr int LINES = ct_lines_of(NC);
-  static constexpr int THREADS = ct_threads_of(NC);
+  static constexpr int LINES = tma_lines_of(NC);
+  static constexpr int THREADS = Ct<NC>::T * LINES;
   static constexpr int ELEMS = LINES * NC;
   static constexpr unsigned BYTES = ELEMS * sizeof(float2);
 };
@@ -309,7 +318,23 @@ static bool get_encoder() {
   return true;
 }
 
-bool tma_supported(int n) { return n == 64 || n == 128 || n == 256; }
+// TMA-fed y pass lengths (the box's line extent is at most 256 elements)
+#define KWB_TMA_COL_SIZES(X)                                                                                   \
+  X(64) X(72) X(75) X(80) X(81) X(90) X(96) X(100) X(108) X(120) X(125) X(128) X(135) X(144) X(150) X(160) \
+  X(162) X(180) X(192) X(200) X(216) X(225) X(240) X(243) X(250) X(256)
+
+bool tma_col_supported(int n) {
+  switch (n) {
+#define KWB_CASE(N) case N:
+    KWB_TMA_COL_SIZES(KWB_CASE)
+#undef KWB_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+bool tma_fused_supported(int n) { return n == 64 || n == 128 || n == 256; }
 
 // Tensor map over a half-spectrum buffer [nz][ny][nxp] (8-byte elements),
 // box {lines, ny or 1, 1 or nz} for transforms along y (yaxis 1) or z (2).
@@ -319,8 +344,8 @@ bool tma_supported(int n) { return n == 64 || n == 128 || n == 256; }
 // multiple of 16 bytes.
 bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n) {
   if (!get_encoder()) return false;
-  const int lines = ct_lines_of(n);
-  if (d.nxp % 2 != 0 || (lines * 8) % 16 != 0) return false;
+  const int lines = tma_lines_of(n);
+  if (d.nxp % 2 != 0 || (lines * 8) % 16 != 0 || lines > 256 || n > 256) return false;
   cuuint64_t dims[3] = {(cuuint64_t)d.nxh, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
   cuuint64_t strides[2] = {(cuuint64_t)d.nxp * 8, (cuuint64_t)d.nxp * d.ny * 8};
   cuuint32_t box[3] = {(cuuint32_t)lines, yaxis == 1 ? (cuuint32_t)d.ny : 1u, yaxis == 2 ? (cuuint32_t)d.nz : 1u};
@@ -381,14 +406,17 @@ static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const 
   return one ? fused_tma_t<NC, FC_SRCK, 1>(a, tw, T, st) : fused_tma_t<NC, FC_SRCK, 0>(a, tw, T, st);
 }
 
-int tma_lines(int n) { return ct_lines_of(n); }
+int tma_lines(int n) { return tma_lines_of(n); }
 
 cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* tw, cudaStream_t st) {
   switch (n) {
-    case 64: return inv ? col_tma_t<64, true>(a, tw, st) : col_tma_t<64, false>(a, tw, st);
-    case 128: return inv ? col_tma_t<128, true>(a, tw, st) : col_tma_t<128, false>(a, tw, st);
-    case 256: return inv ? col_tma_t<256, true>(a, tw, st) : col_tma_t<256, false>(a, tw, st);
-    default: return cudaErrorInvalidValue;
+#define KWB_CASE(N) \
+  case N:           \
+    return inv ? col_tma_t<N, true>(a, tw, st) : col_tma_t<N, false>(a, tw, st);
+    KWB_TMA_COL_SIZES(KWB_CASE)
+#undef KWB_CASE
+    default:
+      return cudaErrorInvalidValue;
   }
 }
 

@@ -62,7 +62,8 @@ cudaError_t launch_medium_maps(float* c0_to_c0sq, float c0_scalar, float* ctau, 
                                float alpha_scalar, double np_per_db, double y, double tan_py, int eos, long long n,
                                cudaStream_t st);
 cudaError_t launch_reciprocal(float* v, long long n, cudaStream_t st);
-bool tma_supported(int n);
+bool tma_col_supported(int n);    // TMA-fed y pass
+bool tma_fused_supported(int n);  // TMA-fed fused last-axis operator
 int tma_lines(int n);
 bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n);
 cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* tw, cudaStream_t st);
@@ -562,8 +563,9 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   // TMA-fed column passes for the compile-time lengths they support
   const char* no_tma = std::getenv("KWAVE_B200_NO_TMA");
   const bool tma_ok = !(no_tma && no_tma[0] == '1');
-  use_tma[1] = tma_ok && tma_supported(d.ny);
-  use_tma[2] = tma_ok && d.dim == 3 && tma_supported(d.nz);
+  // use_tma[1]: the y pass in 3D, the fused last-axis operator in 2D
+  use_tma[1] = tma_ok && (d.dim == 3 ? tma_col_supported(d.ny) : tma_fused_supported(d.ny));
+  use_tma[2] = tma_ok && d.dim == 3 && tma_fused_supported(d.nz);
   for (int s = 0; s < nspec; ++s) {
     if (use_tma[1] && !make_spec_map(&map_y[s], S_buf[s].p, d, 1, d.ny)) use_tma[1] = false;
     if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;

@@ -332,3 +332,32 @@ def test_slabs_on_two_streams_give_identical_results():
                 os.environ[k] = v
     for k in whole:
         np.testing.assert_array_equal(split[k], whole[k], err_msg=k)
+
+
+@pytest.mark.parametrize("ny", [72, 75, 81, 96, 120, 160, 192, 243])
+def test_tma_y_pass_matches_plain_y_pass(ny):
+    """The TMA-fed y pass on 2^a 3^b 5^c lengths other than powers of two
+    (tiles of an even number of lines, so every tile starts 16-byte aligned)
+    gives bit for bit the outputs of the plain column kernels."""
+    import os
+
+    from kwave import _lib
+
+    inp, record, start, _ = case_3d_het(n=(64, ny, 24), nt=10, record=("p", "p_max", "p_rms", "u", "p_final"))
+    tma = _lib.solve(inp, record, start_index=start)
+    old = os.environ.get("KWAVE_B200_NO_TMA")
+    os.environ["KWAVE_B200_NO_TMA"] = "1"
+    try:
+        plain = _lib.solve(inp, record, start_index=start)
+    finally:
+        if old is None:
+            os.environ.pop("KWAVE_B200_NO_TMA", None)
+        else:
+            os.environ["KWAVE_B200_NO_TMA"] = old
+    for k in plain:
+        np.testing.assert_array_equal(tma[k], plain[k], err_msg=k)
+
+
+def test_tma_y_pass_192_against_oracle():
+    inp, record, start, _ = case_3d_het(n=(64, 192, 24), nt=16, record=("p", "p_max", "u", "p_final"))
+    _check(inp, record, TOL)
