@@ -35,6 +35,10 @@ struct TTile {
   static constexpr int THREADS = Ct<NC>::T * LINES;
   static constexpr int ELEMS = LINES * NC;
   static constexpr unsigned BYTES = ELEMS * sizeof(float2);
+  // Stage stride in elements: tensor copies read and write shared memory at
+  // 128-byte aligned addresses, so each stage is padded to a multiple of 128
+  // bytes (a tile of 14 lines of 90 points is 10080 bytes).
+  static constexpr int STRIDE = (int)((BYTES + 127u) / 128u * 128u / sizeof(float2));
 };
 
 __device__ __forceinline__ void tile_coords(int yaxis, int cx, int o, int lines, int& x, int& y, int& z) {
@@ -58,7 +62,7 @@ template <int NC, bool INV>
 __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_constant__ ColTmaArgs a,
                                                                 const float2* __restrict__ tw_g) {
   constexpr int TL = TTile<NC>::LINES;
-  constexpr int E = TTile<NC>::ELEMS;
+  constexpr int E = TTile<NC>::STRIDE;  // stage stride (the tile, padded to 128 bytes)
   constexpr int ST = kColStages;
   extern __shared__ __align__(128) unsigned char smraw[];
   float2* bufs = reinterpret_cast<float2*>(smraw);
@@ -132,6 +136,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
   constexpr int E = TTile<NC>::ELEMS;
   constexpr int TH = TTile<NC>::THREADS;
   static_assert(Ct<NC>::S == 2, "the fused last-axis kernel assumes a two-stage plan");
+  static_assert(TTile<NC>::STRIDE == E, "tile buffers must start at 128-byte aligned addresses");
   extern __shared__ __align__(128) unsigned char smraw[];
   float2* inb = reinterpret_cast<float2*>(smraw);  // 2 input stages
   float2* W = MODE ? nullptr : inb + 2 * E;        // product / inverse-transform buffer (MODE 0)
@@ -368,7 +373,7 @@ static int num_sms() {
 
 template <int NC, bool INV>
 static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t st) {
-  const size_t sm = kColStages * TTile<NC>::BYTES + NC * sizeof(float2) + kColStages * sizeof(uint64_t);
+  const size_t sm = kColStages * TTile<NC>::STRIDE * sizeof(float2) + NC * sizeof(float2) + kColStages * sizeof(uint64_t);
   auto k = k_col_tma<NC, INV>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;
