@@ -41,3 +41,23 @@ def test_malformed_wisdom_is_rejected(tmp_path, text):
         _lib.wisdom_import(str(p))
     with pytest.raises(_lib.KwaveError):
         _lib.wisdom_import(str(tmp_path / "missing.txt"))
+
+
+def test_tuner_and_batch_entry_points_reject_bad_arguments():
+    """Argument checks of kw_tune / kw_batch_* / kw_session_schedule that run
+    before any device work."""
+    import ctypes as C
+
+    st = _lib.KwStatus()
+    sc = _lib.KwSchedule()
+    assert _lib.lib.kw_tune(None, None, C.byref(sc), C.byref(st)) == _lib.KW_ERR_INVALID_ARGUMENT
+    h = C.c_void_p()
+    assert _lib.lib.kw_batch_create(None, 0, C.byref(h), C.byref(st)) == _lib.KW_ERR_INVALID_ARGUMENT
+    arr = (C.c_void_p * 2)(None, None)
+    assert _lib.lib.kw_batch_create(arr, 2, C.byref(h), C.byref(st)) == _lib.KW_ERR_INVALID_ARGUMENT
+    assert b"NULL session" in st.message
+    assert not h.value
+    assert _lib.lib.kw_batch_advance(None, 1, C.byref(st)) == _lib.KW_ERR_INVALID_ARGUMENT
+    assert _lib.lib.kw_batch_graph_launches(None) == 0
+    assert _lib.lib.kw_session_schedule(None, C.byref(sc)) == _lib.KW_ERR_INVALID_ARGUMENT
+    _lib.lib.kw_batch_destroy(None)
