@@ -44,6 +44,7 @@ def _c_layout():
         "kw_output_sizes": [f for f, _ in __import__("kwave._lib", fromlist=["KwOutputSizes"]).KwOutputSizes._fields_],
         "kw_status": ["code", "message"],
         "kw_field": ["data", "numel"],
+        "kw_schedule": [f for f, _ in __import__("kwave._lib", fromlist=["KwSchedule"]).KwSchedule._fields_],
     }
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
     for s, fields in structs.items():
@@ -70,7 +71,7 @@ def test_ctypes_layout_matches_c_header():
     c = _c_layout()
     for name, cls in [("kw_input", _lib.KwInput), ("kw_options", _lib.KwOptions), ("kw_output", _lib.KwOutput),
                       ("kw_output_sizes", _lib.KwOutputSizes), ("kw_status", _lib.KwStatus),
-                      ("kw_field", _lib.KwField)]:
+                      ("kw_field", _lib.KwField), ("kw_schedule", _lib.KwSchedule)]:
         assert C.sizeof(cls) == c[(name, "sizeof")], name
         for f, _ in cls._fields_:
             assert getattr(cls, f).offset == c[(name, f)], f"{name}.{f}"
