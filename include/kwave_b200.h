@@ -288,7 +288,8 @@ void kw_session_destroy(kw_session* s);
  * order.  Sessions with different Nt stop at their own last step.  Work is
  * enqueued after each member's queued work, and each member's later work
  * (kw_session_read, kw_session_sync) waits for it.  Streamed sessions
- * cannot be batched.  Results are bit for bit those of kw_session_advance.
+ * cannot be batched.  The sessions must outlive the batch (destroy the
+ * batch first).  Results are bit for bit those of kw_session_advance.
  */
 typedef struct kw_batch kw_batch;
 int kw_batch_create(kw_session* const* sessions, int n, kw_batch** batch, kw_status* status);

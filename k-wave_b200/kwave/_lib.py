@@ -500,6 +500,8 @@ class Batch:
         self._h = h
 
     def advance(self, n):
+        if any(not getattr(s, "_h", None) for s in self.sessions):
+            raise KwaveError(KW_ERR_INVALID_ARGUMENT, "a session of the batch was closed")
         st = KwStatus()
         _check(lib.kw_batch_advance(self._h, C.c_uint64(int(n)), C.byref(st)), st)
 
