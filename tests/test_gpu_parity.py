@@ -365,3 +365,21 @@ def test_tma_y_pass_matches_plain_y_pass(ny):
 def test_tma_y_pass_192_against_oracle():
     inp, record, start, _ = case_3d_het(n=(64, 192, 24), nt=16, record=("p", "p_max", "u", "p_final"))
     _check(inp, record, TOL)
+
+
+@pytest.mark.parametrize("axis", [0, 1])
+def test_plane_wave_intensity_on_the_gpu(axis):
+    """The reference's analytic plane-wave intensity check (10 W/cm^2 within
+    1 %, kspaceFirstOrder_check_plane_wave_intensity.m:221-233) through the
+    GPU path, and its I_avg against the oracle's."""
+    from kwave import _lib
+    from kwave.simulation import postprocess
+    from test_oracle_pinning import _plane_wave_intensity_case
+
+    (inp, record, start, meta), intensity = _plane_wave_intensity_case(axis)
+    key = "Ix_avg" if axis == 0 else "Iy_avg"
+    gpu = postprocess(_lib.solve(inp, record=record, start_index=start), inp, meta)
+    ora = postprocess(oracle_outputs(inp, record, start, dtype=np.float64), inp, meta)
+    i_gpu = float(np.ravel(gpu[key])[0])
+    assert 100 * abs(intensity - 1e-4 * i_gpu) / intensity <= 1.0
+    assert abs(i_gpu - float(np.ravel(ora[key])[0])) <= TOL * abs(i_gpu)

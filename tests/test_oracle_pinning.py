@@ -7,6 +7,8 @@ identities its unit tests assert (k-Wave/testing/unit/):
   * kspaceFirstOrder3D_compare_binary_and_cuboid_sensor_mask.m;
   * kspaceFirstOrder2D_compare_labelled_and_binary_source_mask.m;
   * kspaceFirstOrder_compare_1D_2D_3D_plane_waves.m (axis symmetry);
+  * kspaceFirstOrder_check_plane_wave_intensity.m (analytic time-averaged
+    intensity within 1 %);
 and the FP32 restatement is checked against the FP64 one (DataCast 'off').
 """
 import numpy as np
@@ -141,3 +143,51 @@ def test_fp32_restatement_tracks_fp64():
     o32 = simulate(inp, rec, dtype=np.float32)
     for k in o64:
         assert rel_l2(o32[k], o64[k]) < 1e-5, k
+
+
+def _plane_wave_intensity_case(axis):
+    """kspaceFirstOrder_check_plane_wave_intensity.m:36-200 in 2D: a 10 MHz
+    plane wave of 10 W/cm^2 time-averaged intensity launched by an additive
+    pressure plane (ramped over 200 samples), recorded two periods at the end
+    of a 3 us run one grid point before the far PML; PML 20 (alpha 2) along
+    the propagation axis, 2 (alpha 0) across it."""
+    nx, nj, dx = 64, 32, 0.05e-3
+    c, rho = 1500.0, 1000.0
+    f0, intensity = 10e6, 10.0  # Hz, W/cm^2
+    strength = np.sqrt(2 * intensity * 1e4 * rho * c)
+    ppp = 30
+    dt = 1.0 / f0 / (2 * ppp)
+    t = np.arange(0.0, 3e-6 + dt / 2, dt)
+    nt = t.size
+    sig = strength * np.sin(2 * np.pi * f0 * t)
+    ramp = (-np.cos(np.arange(200) * np.pi / 200) + 1) / 2
+    sig[:200] *= ramp
+    n = (nx, nj) if axis == 0 else (nj, nx)
+    kg = KWaveGrid(n, (dx, dx))
+    kg.set_time(nt, dt)
+    src_mask, sens_mask = np.zeros(n), np.zeros(n)
+    if axis == 0:
+        src_mask[20, :] = 1
+        sens_mask[nx - 20 - 2, nj // 2 - 1] = 1
+        pml_size, pml_alpha = (20, 2), (2.0, 0.0)
+    else:
+        src_mask[:, 20] = 1
+        sens_mask[nj // 2 - 1, nx - 20 - 2] = 1
+        pml_size, pml_alpha = (2, 20), (0.0, 2.0)
+    sensor = {"mask": sens_mask, "record": ["I", "I_avg"], "record_start_index": nt - 2 * ppp + 1}
+    return prepare(kg, {"sound_speed": c, "density": rho}, {"p_mask": src_mask, "p": sig[None, :]}, sensor,
+                   pml_size=pml_size, pml_alpha=pml_alpha), intensity
+
+
+@pytest.mark.parametrize("axis", [0, 1])
+def test_plane_wave_intensity_matches_the_source(axis):
+    """The reference's analytic intensity check (error <= 1 %,
+    kspaceFirstOrder_check_plane_wave_intensity.m:221-233) on the oracle:
+    the time-averaged intensity at the sensor equals the launched 10 W/cm^2."""
+    from kwave.simulation import postprocess
+
+    (inp, record, start, meta), intensity = _plane_wave_intensity_case(axis)
+    out = postprocess(simulate(inp, record=record, record_start_index=start, dtype=np.float64), inp, meta)
+    i_avg = float(np.ravel(out["Ix_avg" if axis == 0 else "Iy_avg"])[0])
+    err = 100 * abs(intensity - 1e-4 * i_avg) / intensity
+    assert err <= 1.0, err
