@@ -383,3 +383,17 @@ def test_plane_wave_intensity_on_the_gpu(axis):
     i_gpu = float(np.ravel(gpu[key])[0])
     assert 100 * abs(intensity - 1e-4 * i_gpu) / intensity <= 1.0
     assert abs(i_gpu - float(np.ravel(ora[key])[0])) <= TOL * abs(i_gpu)
+
+
+def test_kspace_corrected_source_scaling_on_the_gpu():
+    """The reference's source-scaling check (kspaceFirstOrder2D_check_source_scaling_p.m,
+    error <= 1e-4) with the coarse, k-space corrected run on the GPU and the
+    fine uncorrected reference from the oracle."""
+    from kwave import _lib
+    from test_oracle_pinning import _cw_amplitude, _source_scaling_case, source_scaling_reference_amplitude
+
+    fine = source_scaling_reference_amplitude()
+    (inp, record, start, _), freq, dt = _source_scaling_case(1, "additive")
+    gpu = _lib.solve(inp, record=record, start_index=start)
+    err = abs(_cw_amplitude(gpu["p"], freq, dt) - fine) / fine
+    assert err <= 1e-4, err

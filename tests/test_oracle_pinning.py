@@ -9,6 +9,8 @@ identities its unit tests assert (k-Wave/testing/unit/):
   * kspaceFirstOrder_compare_1D_2D_3D_plane_waves.m (axis symmetry);
   * kspaceFirstOrder_check_plane_wave_intensity.m (analytic time-averaged
     intensity within 1 %);
+  * kspaceFirstOrder2D_check_source_scaling_p.m (k-space corrected source
+    amplitude against a 50x finer uncorrected run, within 1e-4);
 and the FP32 restatement is checked against the FP64 one (DataCast 'off').
 """
 import numpy as np
@@ -191,3 +193,62 @@ def test_plane_wave_intensity_matches_the_source(axis):
     i_avg = float(np.ravel(out["Ix_avg" if axis == 0 else "Iy_avg"])[0])
     err = 100 * abs(intensity - 1e-4 * i_avg) / intensity
     assert err <= 1.0, err
+
+
+def _cw(t, f, ramp_periods=4):
+    """createCWSignals.m: unit sine with a raised-cosine ramp over the first
+    `ramp_periods` periods."""
+    s = np.sin(2 * np.pi * f * t)
+    n = int(round(ramp_periods / f / (t[1] - t[0])))
+    s[:n] *= (-np.cos(np.linspace(0, np.pi, n)) + 1) * 0.5
+    return s
+
+
+def _source_scaling_case(fac, mode):
+    """kspaceFirstOrder2D_check_source_scaling_p.m:36-110: a CW line source
+    (3 points per wavelength, CFL 0.5) on a 64 x 64 grid, the pressure one
+    point before the far PML over the last three periods; `fac` divides the
+    time step (50: the fine reference)."""
+    pml, nx = 20, 64
+    dx = 50e-3 / nx
+    c = 1500.0
+    freq = c / (3 * dx)
+    ppp = round(3 / 0.5)
+    dt = 1 / (ppp * freq)
+    nt = round(50e-6 / dt)
+    dt, nt, ppp = dt / fac, nt * fac, ppp * fac
+    kg = KWaveGrid((nx, nx), (dx, dx))
+    kg.set_time(nt, dt)
+    pm = np.zeros((nx, nx))
+    pm[pml, pml:nx - pml] = 1
+    sm = np.zeros((nx, nx))
+    sm[nx - pml - 1, nx // 2 - 1] = 1
+    src = {"p_mask": pm, "p": _cw(np.arange(nt) * dt, freq)[None, :], "p_mode": mode}
+    sensor = {"mask": sm, "record": ["p"], "record_start_index": nt - 3 * ppp + 1}
+    return prepare(kg, {"sound_speed": c, "density": 1000.0}, src, sensor, pml_size=pml), freq, dt
+
+
+def _cw_amplitude(x, freq, dt):
+    """extractAmpPhase.m with a rectangular window and no padding: the
+    single-sided spectrum at the bin of `freq` (three whole periods)."""
+    x = np.ravel(x)
+    k = int(round(freq * x.size * dt))
+    return 2 * abs(np.fft.fft(x)[k]) / x.size
+
+
+def source_scaling_reference_amplitude():
+    (inp, record, start, _), freq, dt = _source_scaling_case(50, "additive-no-correction")
+    out = simulate(inp, record=record, record_start_index=start, dtype=np.float64)
+    return _cw_amplitude(out["p"], freq, dt)
+
+
+def test_kspace_corrected_source_scaling():
+    """The reference's source-scaling check (error <= 1e-4,
+    kspaceFirstOrder2D_check_source_scaling_p.m:112-118): the k-space
+    corrected additive source at the coarse step gives the amplitude of an
+    uncorrected source at a 50x finer step."""
+    fine = source_scaling_reference_amplitude()
+    (inp, record, start, _), freq, dt = _source_scaling_case(1, "additive")
+    out = simulate(inp, record=record, record_start_index=start, dtype=np.float64)
+    err = abs(_cw_amplitude(out["p"], freq, dt) - fine) / fine
+    assert err <= 1e-4, err
