@@ -9,8 +9,9 @@ identities its unit tests assert (k-Wave/testing/unit/):
   * kspaceFirstOrder_compare_1D_2D_3D_plane_waves.m (axis symmetry);
   * kspaceFirstOrder_check_plane_wave_intensity.m (analytic time-averaged
     intensity within 1 %);
-  * kspaceFirstOrder2D_check_source_scaling_p.m (k-space corrected source
-    amplitude against a 50x finer uncorrected run, within 1e-4);
+  * kspaceFirstOrder2D_check_source_scaling_p.m and _ux.m (k-space
+    corrected source amplitude against a 50x finer uncorrected run, within
+    1e-4);
 and the FP32 restatement is checked against the FP64 one (DataCast 'off').
 """
 import numpy as np
@@ -204,11 +205,12 @@ def _cw(t, f, ramp_periods=4):
     return s
 
 
-def _source_scaling_case(fac, mode):
-    """kspaceFirstOrder2D_check_source_scaling_p.m:36-110: a CW line source
-    (3 points per wavelength, CFL 0.5) on a 64 x 64 grid, the pressure one
-    point before the far PML over the last three periods; `fac` divides the
-    time step (50: the fine reference)."""
+def _source_scaling_case(fac, mode, kind="p"):
+    """kspaceFirstOrder2D_check_source_scaling_p.m:36-110 (kind "p") and
+    _ux.m (kind "ux": the signal divided by c rho as an x-velocity source):
+    a CW line source (3 points per wavelength, CFL 0.5) on a 64 x 64 grid,
+    the pressure one point before the far PML over the last three periods;
+    `fac` divides the time step (50: the fine reference)."""
     pml, nx = 20, 64
     dx = 50e-3 / nx
     c = 1500.0
@@ -223,7 +225,11 @@ def _source_scaling_case(fac, mode):
     pm[pml, pml:nx - pml] = 1
     sm = np.zeros((nx, nx))
     sm[nx - pml - 1, nx // 2 - 1] = 1
-    src = {"p_mask": pm, "p": _cw(np.arange(nt) * dt, freq)[None, :], "p_mode": mode}
+    sig = _cw(np.arange(nt) * dt, freq)[None, :]
+    if kind == "p":
+        src = {"p_mask": pm, "p": sig, "p_mode": mode}
+    else:
+        src = {"u_mask": pm, "ux": sig / (c * 1000.0), "u_mode": mode}
     sensor = {"mask": sm, "record": ["p"], "record_start_index": nt - 3 * ppp + 1}
     return prepare(kg, {"sound_speed": c, "density": 1000.0}, src, sensor, pml_size=pml), freq, dt
 
@@ -236,19 +242,20 @@ def _cw_amplitude(x, freq, dt):
     return 2 * abs(np.fft.fft(x)[k]) / x.size
 
 
-def source_scaling_reference_amplitude():
-    (inp, record, start, _), freq, dt = _source_scaling_case(50, "additive-no-correction")
+def source_scaling_reference_amplitude(kind="p"):
+    (inp, record, start, _), freq, dt = _source_scaling_case(50, "additive-no-correction", kind)
     out = simulate(inp, record=record, record_start_index=start, dtype=np.float64)
     return _cw_amplitude(out["p"], freq, dt)
 
 
-def test_kspace_corrected_source_scaling():
-    """The reference's source-scaling check (error <= 1e-4,
-    kspaceFirstOrder2D_check_source_scaling_p.m:112-118): the k-space
+@pytest.mark.parametrize("kind", ["p", "ux"])
+def test_kspace_corrected_source_scaling(kind):
+    """The reference's source-scaling checks (error <= 1e-4,
+    kspaceFirstOrder2D_check_source_scaling_p.m:112-118, _ux.m): the k-space
     corrected additive source at the coarse step gives the amplitude of an
     uncorrected source at a 50x finer step."""
-    fine = source_scaling_reference_amplitude()
-    (inp, record, start, _), freq, dt = _source_scaling_case(1, "additive")
+    fine = source_scaling_reference_amplitude(kind)
+    (inp, record, start, _), freq, dt = _source_scaling_case(1, "additive", kind)
     out = simulate(inp, record=record, record_start_index=start, dtype=np.float64)
     err = abs(_cw_amplitude(out["p"], freq, dt) - fine) / fine
     assert err <= 1e-4, err
