@@ -12,6 +12,8 @@ identities its unit tests assert (k-Wave/testing/unit/):
   * kspaceFirstOrder2D_check_source_scaling_p.m and _ux.m (k-space
     corrected source amplitude against a 50x finer uncorrected run, within
     1e-4);
+  * kspaceFirstOrder2D_check_nonstaggered_particle_velocity.m (order of the
+    regular- and staggered-grid velocity peaks);
 and the FP32 restatement is checked against the FP64 one (DataCast 'off').
 """
 import numpy as np
@@ -259,3 +261,29 @@ def test_kspace_corrected_source_scaling(kind):
     out = simulate(inp, record=record, record_start_index=start, dtype=np.float64)
     err = abs(_cw_amplitude(out["p"], freq, dt) - fine) / fine
     assert err <= 1e-4, err
+
+
+def test_non_staggered_velocity_lies_between_staggered_points():
+    """kspaceFirstOrder2D_check_nonstaggered_particle_velocity.m:36-101: for
+    an outgoing wave in an absorbing medium, recorded at two adjacent points
+    along x, the peaks of u_x on the regular grid (at the point) and on the
+    staggered grid (half a cell further out) fall in that order: each
+    smaller and no earlier than the one before."""
+    from kwave.simulation import postprocess
+
+    n = (128, 128)
+    kg = KWaveGrid(n, (1e-4, 1e-4))
+    medium = {"sound_speed": 1500.0, "density": 1000.0, "alpha_coeff": 0.75, "alpha_power": 1.5}
+    kg.make_time(1500.0, cfl=0.1, t_end=6e-6)
+    mask = np.zeros(n)
+    mask[64 + 40 - 1, 64 - 1] = 1
+    mask[64 + 40, 64 - 1] = 1
+    p0 = 5 * make_disc(n[0], n[1], 64, 64, 5)
+    inp, record, start, meta = prepare(kg, medium, {"p0": p0}, {"mask": mask, "record": ["p", "u", "u_non_staggered"]})
+    out = postprocess(simulate(inp, record=record, record_start_index=start, dtype=np.float64), inp, meta)
+    uns, us = np.asarray(out["ux_non_staggered"]), np.asarray(out["ux"])
+    seq = [uns[0], us[0], uns[1], us[1]]
+    peaks = [float(s.max()) for s in seq]
+    when = [int(np.argmax(s)) for s in seq]
+    assert peaks[0] > peaks[1] > peaks[2] > peaks[3], peaks
+    assert when[0] <= when[1] <= when[2] <= when[3], when
