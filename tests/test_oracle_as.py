@@ -100,3 +100,43 @@ def test_front_end_builds_axisymmetric_datasets():
     ux, _, _, _ = prepare(kg, {"sound_speed": 1500.0}, {"u_mask": np.ones((40, 20)), "ux": np.ones((1, 5))},
                           {"mask": np.ones((40, 20))}, pml_size=5, axisymmetric=True)
     assert ux["ux_source_flag"] == 5 and ux["axisymmetric_flag"] == 1
+
+
+def test_piston_on_axis_pressure_matches_the_closed_form():
+    """kspaceFirstOrderAS_piston_analytical.m:36-140: a 1 MHz CW piston of
+    5 mm radius on the axis of an axisymmetric grid (12 points per
+    wavelength, CFL 0.25, PML outside the grid) gives the on-axis steady
+    amplitude 2 P |sin(k (sqrt(x^2 + a^2) - x) / 2)| within 1 % (Linf over the
+    axis, relative to its maximum).  PML 20 points stands in for the
+    reference's 'auto' size."""
+    from kwave.simulation import postprocess, prepare
+    from kwave.utils import KWaveGrid
+    from test_oracle_pinning import _cw
+
+    c0, rho0, f0, a_src, mag = 1500.0, 1000.0, 1e6, 5e-3, 1e6
+    ppw, cfl = 12, 0.25
+    dx = c0 / (ppw * f0)
+    nx, ny = int(2 * round(32e-3 / dx / 2)), int(2 * round(10e-3 / dx / 2))
+    ppp = round(ppw / cfl)
+    dt = 1 / (ppp * f0)
+    nt = round(40e-6 / dt)
+    kg = KWaveGrid((nx, ny), (dx, dx))
+    kg.set_time(nt, dt)
+    rgp = round(a_src / dx)
+    pm = np.zeros((nx, ny))
+    pm[0, :rgp] = 1
+    sm = np.zeros((nx, ny))
+    sm[1:, 0] = 1  # the axis
+    src = {"p_mask": pm, "p": mag * _cw(np.arange(nt) * dt, f0)[None, :]}
+    sensor = {"mask": sm, "record": ["p"], "record_start_index": nt - 3 * ppp + 1}
+    inp, rec, start, meta = prepare(kg, {"sound_speed": c0, "density": rho0}, src, sensor,
+                                    pml_size=(20, 20), pml_inside=False, axisymmetric=True)
+    p = np.asarray(postprocess(simulate_as(inp, record=rec, record_start_index=start, dtype=np.float64),
+                               inp, meta)["p"])
+    k = int(round(f0 * p.shape[1] * dt))
+    amp = 2 * np.abs(np.fft.fft(p, axis=1)[:, k]) / p.shape[1]
+    x = np.arange(1, nx) * dx
+    kk, a = 2 * np.pi * f0 / c0, (rgp - 0.5) * dx
+    ref = mag * np.abs(2 * np.sin((kk * np.sqrt(x ** 2 + a ** 2) - kk * x) / 2))
+    err = 100 * np.max(np.abs(ref - amp)) / ref.max()
+    assert err <= 1.0, err
