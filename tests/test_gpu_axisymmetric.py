@@ -158,3 +158,40 @@ def test_axial_velocity_sources(mode):
     base.update(ux_source_flag=35, u_source_mode=mode, u_source_many=many, u_source_index=idx, ux_source_input=s)
     gpu = _check(base, ("p", "u", "p_max", "p_final"), TOL)
     assert np.abs(gpu["p"]).max() > 0
+
+
+def test_piston_on_axis_pressure_on_the_gpu():
+    """The reference's analytic piston check (kspaceFirstOrderAS_piston_analytical.m,
+    Linf <= 1 %) through the GPU path: PML 22 axial / 20 radial outside the
+    grid, so the expanded grid is 300 x 4 * 100 points."""
+    from kwave import _lib
+    from kwave.simulation import postprocess, prepare
+    from kwave.utils import KWaveGrid
+    from test_oracle_pinning import _cw
+
+    c0, rho0, f0, a_src, mag = 1500.0, 1000.0, 1e6, 5e-3, 1e6
+    ppw, cfl = 12, 0.25
+    dx = c0 / (ppw * f0)
+    nx, ny = int(2 * round(32e-3 / dx / 2)), int(2 * round(10e-3 / dx / 2))
+    ppp = round(ppw / cfl)
+    dt = 1 / (ppp * f0)
+    nt = round(40e-6 / dt)
+    kg = KWaveGrid((nx, ny), (dx, dx))
+    kg.set_time(nt, dt)
+    rgp = round(a_src / dx)
+    pm = np.zeros((nx, ny))
+    pm[0, :rgp] = 1
+    sm = np.zeros((nx, ny))
+    sm[1:, 0] = 1
+    src = {"p_mask": pm, "p": mag * _cw(np.arange(nt) * dt, f0)[None, :]}
+    sensor = {"mask": sm, "record": ["p"], "record_start_index": nt - 3 * ppp + 1}
+    inp, rec, start, meta = prepare(kg, {"sound_speed": c0, "density": rho0}, src, sensor,
+                                    pml_size=(22, 20), pml_inside=False, axisymmetric=True)
+    assert (int(inp["Nx"]), int(inp["Ny"])) == (300, 100)
+    p = np.asarray(postprocess(_lib.solve(inp, record=rec, start_index=start), inp, meta)["p"])
+    k = int(round(f0 * p.shape[1] * dt))
+    amp = 2 * np.abs(np.fft.fft(p, axis=1)[:, k]) / p.shape[1]
+    x = np.arange(1, nx) * dx
+    kk, a = 2 * np.pi * f0 / c0, (rgp - 0.5) * dx
+    ref = mag * np.abs(2 * np.sin((kk * np.sqrt(x ** 2 + a ** 2) - kk * x) / 2))
+    assert 100 * np.max(np.abs(ref - amp)) / ref.max() <= 1.0
