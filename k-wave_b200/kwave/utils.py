@@ -190,6 +190,11 @@ def cart_linear_weights(kgrid: KWaveGrid, cart):
         if f[a].min() < -1e-9 or f[a].max() > kgrid.N[a] - 1 + 1e-9:
             raise ValueError("Cartesian points must lie within the grid defined by kgrid.")
     f = np.clip(f, 0, np.array(kgrid.N, dtype=np.float64)[:, None] - 1)
+    # coordinates a few ulps from a grid line (points given on grid nodes,
+    # whose coordinates carry the rounding of the grid vectors) are put on
+    # it, so a point on a node takes that node's value exactly
+    near = np.abs(f - np.round(f)) < 1e-9
+    f[near] = np.round(f[near])
     i0 = np.minimum(np.floor(f).astype(np.int64), np.array(kgrid.N)[:, None] - 2)
     t = f - i0  # in [0, 1]
     order = np.argsort(-t, axis=0, kind="stable")  # axes by decreasing fraction

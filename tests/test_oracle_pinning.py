@@ -14,6 +14,7 @@ identities its unit tests assert (k-Wave/testing/unit/):
     1e-4);
   * kspaceFirstOrder2D_check_nonstaggered_particle_velocity.m (order of the
     regular- and staggered-grid velocity peaks);
+  * kspaceFirstOrder2D_compare_binary_and_cartesian_sensor_mask.m (1e-14);
 and the FP32 restatement is checked against the FP64 one (DataCast 'off').
 """
 import numpy as np
@@ -287,3 +288,54 @@ def test_non_staggered_velocity_lies_between_staggered_points():
     when = [int(np.argmax(s)) for s in seq]
     assert peaks[0] > peaks[1] > peaks[2] > peaks[3], peaks
     assert when[0] <= when[1] <= when[2] <= when[3], when
+
+
+def test_binary_and_cartesian_sensors_agree():
+    """kspaceFirstOrder2D_compare_binary_and_cartesian_sensor_mask.m:36-150:
+    Cartesian sensor points placed on grid nodes give, with linear
+    interpolation and with the nearest-point mapping, the outputs of the
+    same points as a binary mask reordered to the points' order (relative
+    max error 1e-14), for p, u, u on the regular grid, their max / min / rms
+    and the intensity.  A one-point-wide ring (a disc less a smaller disc)
+    stands in for makeCircle."""
+    from kwave.simulation import postprocess
+
+    n = (128, 128)
+    dx = 25e-3 / n[0]
+    kg = KWaveGrid(n, (dx, dx))
+    c = 1500 * np.ones(n)
+    c[n[0] // 2 - 1:, :] = 2000
+    rho = 1000 * np.ones(n)
+    rho[n[0] // 2 - 1:, :] = 1200
+    kg.make_time(c)
+    p0 = np.zeros(n)
+    p0[21, n[1] // 4 - 1:3 * n[1] // 4] = 1
+    ring = make_disc(n[0], n[1], n[0] // 2, n[1] // 2, n[0] // 2 - 10) - make_disc(
+        n[0], n[1], n[0] // 2, n[1] // 2, n[0] // 2 - 11)
+    jj, ii = np.nonzero(ring.T)  # MATLAB find order: x fastest
+    cart = np.stack([kg.vec(0)[ii], kg.vec(1)[jj]])
+    record = ["p", "p_max", "p_min", "p_rms", "u", "u_max", "u_min", "u_rms", "u_non_staggered", "I", "I_avg"]
+    medium = {"sound_speed": c, "density": rho}
+    runs = {}
+    for name, mask, interp in (("linear", cart, "linear"), ("nearest", cart, "nearest"), ("binary", cart, None)):
+        kw = {"cart_interp": interp} if interp else {}
+        if interp is None:
+            from kwave.utils import cart2grid
+
+            mask = cart2grid(kg, cart)[0]
+        inp, rec, start, meta = prepare(kg, medium, {"p0": p0}, {"mask": mask, "record": list(record)}, **kw)
+        runs[name] = postprocess(simulate(inp, record=rec, record_start_index=start, dtype=np.float64), inp, meta)
+        if interp is None:  # binary outputs come in grid order: reorder to the points' order
+            from kwave.utils import reorder_binary_sensor_data
+
+            order = cart2grid(kg, cart)[1]
+            runs[name] = {k: (reorder_binary_sensor_data(np.asarray(v), order) if np.ndim(v) and
+                              np.shape(v)[0] == cart.shape[1] else v) for k, v in runs[name].items()}
+    keys = [k for k in runs["binary"] if k in runs["linear"] and k in runs["nearest"]]
+    assert {"p", "p_max", "ux", "uy_rms", "ux_non_staggered", "Ix_avg"} <= set(keys), keys
+    for k in keys:
+        b = np.asarray(runs["binary"][k], dtype=np.float64)
+        for other in ("linear", "nearest"):
+            o = np.asarray(runs[other][k], dtype=np.float64)
+            err = np.max(np.abs(o - b)) / np.max(np.abs(b))
+            assert err <= 1e-14, (k, other, err)
