@@ -10,6 +10,14 @@ simulation resident in HBM (kw_session_advance, CUDA events on the session's
 stream); `e2e` is a whole solve through the C ABI (kw_solve) from pinned
 host buffers, host<->device copies included.  Every field (1.1 GB working
 set) is larger than the 126 MB L2, so no flush is needed between steps.
+Before anything is timed, kw_tune picks the step's launch schedule for the
+grid (z slabs, streams; reported in config.schedule); the session and the
+solves use it.
+
+The `batched` object times 48 uneven 3D simulations one at a time, as
+sessions interleaved on their own streams, and as one kw_batch (each step of
+all 48 one CUDA graph launch), plus the plain drop-in (the solver binary per
+simulation); `served` a Poisson request stream through the server.
 
 Multi-GPU: each rank runs its own independent simulation ("replicas
 only": one simulation does not shard), so `value` sums over ranks.
