@@ -11,7 +11,7 @@ stream); `e2e` is a whole solve through the C ABI (kw_solve) from pinned
 host buffers, host<->device copies included.  Every field (1.1 GB working
 set) is larger than the 126 MB L2, so no flush is needed between steps.
 Before anything is timed, kw_tune picks the step's launch schedule for the
-grid (z slabs, streams; reported in config.schedule); the session and the
+grid (z slabs, streams; reported in `schedule`); the session and the
 solves use it.
 
 The `batched` object times 48 uneven 3D simulations one at a time, as
@@ -355,37 +355,70 @@ def served_sample(n_requests, budget_gb=150.0, chunk=0):
                       "written, binary run, output file read), one at a time"}
 
 
+def workload_config(grid, nt, world):
+    """The `config` object of both arms (same keys, same values)."""
+    return {"workload": WORKLOAD, "grid": [int(g) for g in grid], "Nt": int(nt),
+            "parallelism": f"replicas{world}", "l2": "working set 1.1 GB > 126 MB L2, no flush needed"}
+
+
+def mapped_repo_libraries():
+    """Shared objects of this repository mapped into the process."""
+    try:
+        with open("/proc/self/maps") as f:
+            return sorted({ln.split()[-1] for ln in f if ln.rstrip().endswith(".so") and ROOT in ln})
+    except OSError:
+        return []
+
+
+class _SampleDone(Exception):
+    pass
+
+
 def run_reference(args):
+    """The reference arm: the reference algorithm on the host cores (the
+    oracle port, numpy + scipy.fft on every host thread), the same workload,
+    metric and config as the GPU arm.  `--warmup` untimed time steps, then up
+    to `--steps` timed ones, stopping early once the timed steps pass
+    REF_TIMED_S seconds (the steps actually timed are reported)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     inp, record, start = build_input(args.n, args.nt)
     from oracle.kspace_oracle import simulate
 
     npts = args.n ** 3
-    # bounded sample: warm-up steps plus timed steps, capped at ~3 minutes
+    w, k_req = max(0, args.warmup), max(1, args.steps)
     stamps = []
-    w = max(1, min(args.warmup, 3))
     t0 = time.perf_counter()
-    probe = []
-    simulate(inp, record=record, dtype=np.float32, workers=-1, max_steps=w + 1,
-             on_step=lambda t: probe.append(time.perf_counter()))
-    per_est = probe[-1] - probe[-2]
-    k = max(1, min(args.steps, int(150.0 / max(per_est, 1e-3))))
-    simulate(inp, record=record, dtype=np.float32, workers=-1, max_steps=w + k,
-             on_step=lambda t: stamps.append(time.perf_counter()))
-    per = (stamps[-1] - stamps[w - 1]) / k
+    REF_TIMED_S = 180.0
+
+    a = max(w, 1) - 1  # stamps[a] closes the last untimed step (one anchoring step when --warmup 0)
+
+    def on_step(t):
+        stamps.append(time.perf_counter())
+        if len(stamps) - 1 - a >= 1 and stamps[-1] - stamps[a] > REF_TIMED_S:
+            raise _SampleDone()
+
+    try:
+        simulate(inp, record=record, dtype=np.float32, workers=-1, max_steps=a + 1 + k_req, on_step=on_step)
+    except _SampleDone:
+        pass
+    k = len(stamps) - 1 - a
+    per = (stamps[-1] - stamps[a]) / k
     value = npts / per
     cores = os.cpu_count()
+    so = mapped_repo_libraries()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": k, "warmup": w, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "Nt": args.nt},
+        "config": workload_config((args.n,) * 3, args.nt, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"time steps {w + 1}..{w + k} of the {args.n}^3 run, numpy/scipy.fft "
-                                   f"workers={cores}; MATLAB reference not installable here"},
+                         "sample": f"time steps {a + 2}..{a + 1 + k} of the {args.n}^3 run after {a + 1} untimed, "
+                                   f"numpy/scipy.fft workers={cores}; MATLAB reference not installable here"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "repo_libraries_mapped": so,
         "wall_s": time.perf_counter() - t0,
     }
     print(json.dumps(line), flush=True)
@@ -492,13 +525,12 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [int(inp["Nx"]), int(inp["Ny"]), int(inp["Nz"])], "Nt": int(inp["Nt"]),
-                   "parallelism": f"replicas{world}", "l2": "working set 1.1 GB > 126 MB L2, no flush needed",
-                   "schedule": {"used": {k: sched_used[k] for k in ("slab_planes", "streams", "row_lines", "col_lines")},
-                                "tuned": sched}},
+        "config": workload_config((inp["Nx"], inp["Ny"], inp["Nz"]), inp["Nt"], world),
+        "schedule": {"used": {k: sched_used[k] for k in ("slab_planes", "streams", "row_lines", "col_lines")},
+                     "tuned": sched},
         "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes(inp), "d2h_bytes_per_step": d2h,
                  "note": f"one e2e step = one whole {int(inp['Nt'])}-step solve via kw_solve, pinned host buffers"
-                         + ("; launch schedule tuned once beforehand (kw_tune, config.schedule.tuned.tune_s)"
+                         + ("; launch schedule tuned once beforehand (kw_tune, schedule.tuned.tune_s)"
                             if sched else "")}
                 if e2e_value else None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

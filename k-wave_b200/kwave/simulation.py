@@ -21,7 +21,6 @@ from __future__ import annotations
 import numpy as np
 import scipy.fft as sfft
 
-from . import _lib
 from .transducer import KWaveTransducer, transducer_source_datasets
 from .utils import KWaveGrid, cart2grid, cart_linear_weights, reorder_binary_sensor_data, smooth
 
@@ -417,6 +416,8 @@ def postprocess(out: dict, inp: dict, meta: dict):
 def kspace_first_order(kgrid: KWaveGrid, medium: dict, source: dict, sensor: dict, *, device=-1, **options):
     """Run a simulation (the G-suffixed drop-in path) and return sensor_data
     as the reference does."""
+    from . import _lib  # the CUDA library is mapped here, on the first solve
+
     inp, record, start, meta = prepare(kgrid, medium, source, sensor, **options)
     out = _lib.solve(inp, record=record, start_index=start, device=device)
     return postprocess(out, inp, meta)

@@ -23,8 +23,10 @@ try:
     MATLAB_73 = os.path.join(os.path.dirname(_sm.__file__), "tests", "data", "testhdf5_7.4_GLNX86.mat")
 except ImportError:
     pass
-# a chunked + deflated MATLAB 7.3 file of the reference's example data
-REF_EXAMPLE = os.path.join("/root/reference", "k-Wave", "examples", "EXAMPLE_shepp_logan.mat")
+# a chunked + deflated MATLAB 7.3 file of the reference's example data, read
+# when KWAVE_B200_REFERENCE_TREE names a checkout of the reference (k-Wave/...)
+_REF_TREE = os.environ.get("KWAVE_B200_REFERENCE_TREE")
+REF_EXAMPLE = os.path.join(_REF_TREE, "k-Wave", "examples", "EXAMPLE_shepp_logan.mat") if _REF_TREE else None
 
 
 def _lib():
@@ -127,7 +129,7 @@ def test_matlab_written_file():
         assert f.attrs("/testdouble")["MATLAB_class"] == "double"
 
 
-@pytest.mark.skipif(not os.path.exists(REF_EXAMPLE), reason="reference example data absent")
+@pytest.mark.skipif(not (REF_EXAMPLE and os.path.exists(REF_EXAMPLE)), reason="KWAVE_B200_REFERENCE_TREE unset or its example data absent")
 def test_chunked_deflated_matlab_file():
     """Chunked (B-tree v1) + deflate: both readers agree bit for bit on the
     modified Shepp-Logan phantom, whose intensities are 0, .1, .2, .3, .4, 1."""
