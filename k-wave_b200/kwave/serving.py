@@ -15,8 +15,16 @@ alone.
   memory is admitted as soon as a finished one frees enough), and records
   each request's time to solution.
 
-Both take a ``factory`` that builds a session from a request, so the
-scheduling logic can be exercised without a GPU.
+Several GPUs: both take a list of devices.  Simulations are independent, so
+they are placed whole on one device each, with no collective between
+devices: the server puts each request on the device with the most free
+budget (the reference's per-run device choice, ``-g`` in
+kspaceFirstOrder3DC.m:308-325, made by the scheduler), and the batch runner
+deals its simulations out largest first to the least loaded device.
+
+Both take a ``factory`` that builds a session from a request (inputs,
+record, start index, device), so the scheduling logic can be exercised
+without a GPU.
 """
 from __future__ import annotations
 
@@ -117,6 +125,7 @@ class Request:
     result: dict = None
     error: str = None
     nbytes: int = 0
+    device: int = None
 
     @property
     def latency(self):
@@ -127,18 +136,34 @@ class Request:
         return int(self.inp["Nx"]) * int(self.inp["Ny"]) * int(self.inp["Nz"]) * int(self.inp["Nt"])
 
 
-def run_batch(inputs, record=("p",), chunk=25, factory=gpu_session, sync=True, mode="auto"):
+def place_on_devices(inputs, devices):
+    """Device of each simulation: largest first (grid-point-steps) to the
+    device with the least work so far, so the devices finish together."""
+    load = [0] * len(devices)
+    out = [None] * len(inputs)
+    work = lambda inp: int(inp["Nx"]) * int(inp["Ny"]) * int(inp["Nz"]) * int(inp["Nt"])
+    for i in sorted(range(len(inputs)), key=lambda i: -work(inputs[i])):
+        k = min(range(len(devices)), key=lambda k: (load[k], k))
+        load[k] += work(inputs[i])
+        out[i] = devices[k]
+    return out
+
+
+def run_batch(inputs, record=("p",), chunk=25, factory=gpu_session, sync=True, mode="auto", devices=(-1,)):
     """Advance every simulation in `inputs` to its last step and return their
     outputs in order.
 
-    mode "graph": one kw_batch advances them all, each time step of every
-    simulation one CUDA graph launch (library sessions only; measured a
-    little faster than streams on 48 uneven 3D grids).  mode "streams": the
-    sessions are interleaved in chunks of `chunk` steps, each session's steps
-    on its own stream, so the device runs them concurrently.  "auto" takes
-    "graph" for library sessions and "streams" for any other session type.
-    Work is only enqueued until the outputs are read."""
-    sessions = [factory(inp, record) for inp in inputs]
+    mode "graph": one kw_batch per device advances its simulations, each
+    time step of all of them one CUDA graph launch (library sessions only;
+    measured a little faster than streams on 48 uneven 3D grids).  mode
+    "streams": the sessions are interleaved in chunks of `chunk` steps, each
+    session's steps on its own stream, so the device runs them concurrently.
+    "auto" takes "graph" for library sessions and "streams" for any other
+    session type.  `devices`: the GPUs to spread the simulations over
+    (place_on_devices); -1 is the current device.  Work is only enqueued
+    until the outputs are read."""
+    where = place_on_devices(inputs, list(devices))
+    sessions = [factory(inp, record, 1, dev) for inp, dev in zip(inputs, where)]
     try:
         if mode == "auto":
             try:
@@ -151,12 +176,17 @@ def run_batch(inputs, record=("p",), chunk=25, factory=gpu_session, sync=True, m
         if mode == "graph":
             from ._lib import Batch
 
-            b = Batch(sessions)
+            groups = {}
+            for s, dev in zip(sessions, where):
+                groups.setdefault(dev, []).append(s)
+            batches = [Batch(g) for g in groups.values()]
             try:
                 for _ in range(0, max(int(inp["Nt"]) for inp in inputs), chunk):
-                    b.advance(chunk)
+                    for b in batches:  # each device's batch runs while the host feeds the next
+                        b.advance(chunk)
             finally:
-                b.close()
+                for b in batches:
+                    b.close()
         elif mode == "streams":
             left = [int(inp["Nt"]) for inp in inputs]
             while any(left):
@@ -179,7 +209,7 @@ def run_plain(inputs, record=("p",), factory=gpu_session):
     before the next starts."""
     out = []
     for inp in inputs:
-        s = factory(inp, record)
+        s = factory(inp, record, 1, -1)
         try:
             s.advance(int(inp["Nt"]))
             out.append(s.read())
@@ -200,7 +230,9 @@ def library_sizer(r):
 class Server:
     """Admits requests by device-memory budget and interleaves their steps.
 
-    `budget_bytes` bounds the summed estimate of admitted sessions.  Each
+    `budget_bytes` bounds the summed estimate of the sessions admitted to
+    each device in `devices` (device ordinals, -1 for the current device);
+    a request goes to the device with the most free budget.  Each
     session is fed chunks of steps (`chunk`, or if 0 about `chunk_seconds`
     of device time at `step_rate` grid-point-steps/s) while fewer than
     `max_queued` of its chunks are still running, so its stream never runs
@@ -211,6 +243,7 @@ class Server:
     `clock` / `sleep` are the time source (replaceable by a simulated clock
     in tests)."""
     budget_bytes: int = 150 * 10**9
+    devices: tuple = (-1,)
     chunk: int = 0
     max_queued: int = 3
     chunk_seconds: float = 4e-3
@@ -233,31 +266,36 @@ class Server:
                 r.error = f"needs {r.nbytes} B of device memory, more than the {self.budget_bytes} B budget"
         queue = [r for r in pending if r.error is None]
         levels = self._priority_levels() if self.priorities else None
-        active = []  # [request, session, steps queued, chunk]
-        used = 0
+        active = []  # [request, session, steps queued, chunk, device slot]
+        used = [0] * len(self.devices)
         t0 = self.clock()
         now = lambda: self.clock() - t0
         while queue or active:
             progressed = False
-            # admission: arrived requests, first come first served, while they fit
-            while queue and queue[0].arrival <= now() and used + queue[0].nbytes <= self.budget_bytes:
+            # admission: arrived requests, first come first served, each on
+            # the device with the most free budget, while one has room
+            while queue and queue[0].arrival <= now():
+                k = self.place(queue[0].nbytes, used)
+                if k is None:
+                    break
                 r = queue.pop(0)
                 try:
-                    sess = self.factory(r.inp, r.record, r.start_index)
+                    sess = self.factory(r.inp, r.record, r.start_index, self.devices[k])
                 except Exception as e:  # noqa: BLE001 - reported per request
                     r.error = str(e)
                     continue
                 if levels and hasattr(sess, "set_priority"):
                     sess.set_priority(self._priority(r, levels))
                 r.admitted = now()
-                used += r.nbytes
-                active.append([r, sess, 0, self._chunk(r)])
-                self.log.append(("admit", r.tag, r.admitted, used))
+                r.device = self.devices[k]
+                used[k] += r.nbytes
+                active.append([r, sess, 0, self._chunk(r), k])
+                self.log.append(("admit", r.tag, r.admitted, used[k], self.devices[k]))
                 progressed = True
             # interleave: top up each session's stream with its next chunk,
             # collect the sessions whose last step has finished
             for a in list(active):
-                r, sess, queued, chunk = a
+                r, sess, queued, chunk, k = a
                 nt = int(r.inp["Nt"])
                 if queued < nt:
                     if sess.in_flight() < self.max_queued:
@@ -274,13 +312,22 @@ class Server:
                     finally:
                         sess.close()
                     r.finished = now()
-                    used -= r.nbytes
+                    used[k] -= r.nbytes
                     active.remove(a)
-                    self.log.append(("finish", r.tag, r.finished, used))
+                    self.log.append(("finish", r.tag, r.finished, used[k], self.devices[k]))
                     progressed = True
             if not progressed:
                 self.sleep(self.idle_sleep_s)
         return pending
+
+    def place(self, nbytes, used):
+        """Slot of the device with the most free budget that fits `nbytes`
+        (the lowest slot on ties), or None when none has room."""
+        best = None
+        for k, u in enumerate(used):
+            if u + nbytes <= self.budget_bytes and (best is None or u < used[best]):
+                best = k
+        return best
 
     def _chunk(self, r):
         if self.chunk:
@@ -316,7 +363,7 @@ def serve_plain(requests, factory=gpu_session, clock=time.perf_counter, sleep=ti
         while clock() - t0 < r.arrival:
             sleep(min(1e-3, r.arrival - (clock() - t0)))
         r.admitted = clock() - t0
-        sess = factory(r.inp, r.record, r.start_index)
+        sess = factory(r.inp, r.record, r.start_index, -1)
         try:
             sess.advance(int(r.inp["Nt"]))
             r.result = sess.read()

@@ -103,3 +103,32 @@ def test_dropin_sessions_give_the_same_results():
         s.advance(int(inp["Nt"]))
         _same(r.result, s.read())
         s.close()
+
+
+def test_server_over_two_device_slots_gives_solo_results():
+    """Placement across devices, with both slots naming device 0 (this run
+    has one GPU): requests are spread over the two budgets and each result is
+    still the solo result."""
+    from kwave import _lib, serving
+
+    cases = _cases()
+    reqs = [serving.Request(inp=inp, record=rec, arrival=0.0, tag=i) for i, (inp, rec) in enumerate(cases)]
+    sizes = [serving.library_sizer(r) for r in reqs]
+    srv = serving.Server(budget_bytes=max(sizes) + min(sizes), chunk=8, devices=(0, 0))
+    out = srv.serve(reqs)
+    slots = [e for e in srv.log if e[0] == "admit"]
+    assert len(slots) == len(cases)
+    for r, (inp, rec) in zip(sorted(out, key=lambda r: r.tag), cases):
+        assert r.error is None, r.error
+        assert r.device == 0
+        _same(r.result, _lib.solve(inp, rec))
+
+
+def test_run_batch_over_two_device_slots_matches_plain():
+    from kwave import serving
+
+    inputs = [case_2d_p0(n=(48, 48), nt=40)[0], case_2d_p0(n=(60, 50), nt=25)[0], case_2d_p0(n=(32, 64), nt=31)[0]]
+    a = serving.run_batch(inputs, ("p", "p_max"), chunk=9, devices=(0, 0))
+    b = serving.run_plain(inputs, ("p", "p_max"))
+    for x, y in zip(a, b):
+        _same(x, y)

@@ -50,16 +50,17 @@ def _req(tag, nt=100, arrival=0.0, nbytes=1):
                            tag=tag)
 
 
-def _server(clock, budget, trace=None, chunk=10):
+def _server(clock, budget, trace=None, chunk=10, devices=(-1,)):
     made = []
 
-    def factory(inp, record, start_index=1):
+    def factory(inp, record, start_index=1, device=-1):
         s = FakeSession(clock, inp, record, start_index, trace=trace)
+        s.device = device
         made.append(s)
         return s
 
     srv = serving.Server(budget_bytes=budget, chunk=chunk, factory=factory, sizer=lambda r: r.inp["bytes"],
-                         priorities=False, clock=clock.now, sleep=clock.sleep, idle_sleep_s=1e-4)
+                         priorities=False, clock=clock.now, sleep=clock.sleep, idle_sleep_s=1e-4, devices=devices)
     return srv, made
 
 
@@ -122,7 +123,7 @@ def test_admission_waits_for_arrival_times():
 
 def test_batch_and_plain_return_outputs_in_order():
     clock = Clock()
-    mk = lambda inp, record, start_index=1: FakeSession(clock, inp, record, cost=0.0)
+    mk = lambda inp, record, start_index=1, device=-1: FakeSession(clock, inp, record, cost=0.0)
     inputs = [{"Nx": 4, "Ny": 4, "Nz": 1, "Nt": nt, "tag": i} for i, nt in enumerate((30, 7, 55))]
     a = serving.run_batch(inputs, ("p",), chunk=10, factory=mk)
     b = serving.run_plain(inputs, ("p",), factory=mk)
@@ -160,3 +161,59 @@ def test_priority_levels_follow_job_size_and_chunks_follow_grid_size():
     srv = serving.Server(chunk=0, chunk_seconds=4e-3, step_rate=1e10)
     assert srv._chunk(small) == 200 and srv._chunk(big) == 5
     assert serving.Server(chunk=17)._chunk(big) == 17
+
+
+def test_requests_go_to_the_device_with_the_most_free_budget():
+    clock = Clock()
+    srv, made = _server(clock, budget=4, devices=(0, 1))
+    reqs = [_req(0, nbytes=3), _req(1, nbytes=2), _req(2, nbytes=2), _req(3, nbytes=1)]
+    out = srv.serve(reqs)
+    assert all(r.error is None and int(r.result["p"][0]) == r.tag for r in out)
+    # 0 -> device 0 (both empty, lowest first); 1 -> device 1 (4 free against 1);
+    # 2 -> device 1 (2 free against 1); 3 -> device 0 (1 free against 0)
+    assert [r.device for r in out] == [0, 1, 1, 0]
+    assert [s.device for s in made] == [0, 1, 1, 0]
+    for dev in (0, 1):  # no device ever holds more than its budget
+        assert max(e[3] for e in srv.log if e[0] == "admit" and e[4] == dev) <= 4
+
+
+def test_a_request_waits_until_some_device_has_room():
+    clock = Clock()
+    srv, _ = _server(clock, budget=3, devices=(0, 1))
+    reqs = [_req(0, nbytes=3, nt=200), _req(1, nbytes=3, nt=100), _req(2, nbytes=3, nt=10)]
+    out = srv.serve(reqs)
+    assert [r.device for r in out[:2]] == [0, 1]
+    # the third fits nowhere until the shorter of the first two finishes, and takes its device
+    assert out[2].admitted >= out[1].finished and out[2].device == 1
+
+
+def test_two_devices_halve_the_makespan_of_equal_jobs():
+    def makespan(devices):
+        clock = Clock()
+        srv, _ = _server(clock, budget=1, devices=devices)
+        out = srv.serve([_req(i, nt=100) for i in range(4)])
+        return max(r.finished for r in out)
+
+    one, two = makespan((0,)), makespan((0, 1))
+    assert two == pytest.approx(one / 2, rel=0.05)
+
+
+def test_batch_placement_balances_work_largest_first():
+    inputs = [{"Nx": n, "Ny": n, "Nz": n, "Nt": 10} for n in (64, 128, 96, 128, 64)]
+    where = serving.place_on_devices(inputs, [0, 1])
+    work = lambda i: inputs[i]["Nx"] ** 3
+    load = {d: sum(work(i) for i in range(5) if where[i] == d) for d in (0, 1)}
+    # the two 128^3 jobs land on different devices, the rest fill the lighter one
+    assert where[1] != where[3]
+    assert abs(load[0] - load[1]) <= 96 ** 3
+    clock = Clock()
+    made = []
+
+    def mk(inp, record, start_index=1, device=-1):
+        s = FakeSession(clock, dict(inp, tag=len(made)), record, cost=0.0)
+        s.device = device
+        made.append(s)
+        return s
+
+    serving.run_batch([dict(i) for i in inputs], ("p",), chunk=5, factory=mk, devices=(0, 1))
+    assert [s.device for s in made] == where
