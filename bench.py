@@ -374,6 +374,53 @@ class _SampleDone(Exception):
     pass
 
 
+def fft_sample(grids=((256, 256, 256), (120, 150, 90), (160, 135, 192)), reps=20, warmup=3):
+    """The solver's own FFT passes (kw_fft3d: x row transform, y and z column
+    passes) against cuFFT (torch.fft.rfftn / irfftn, FP32, unnormalised
+    inverse) on the same grids: ms per 3D R2C and C2R, and ms of each of our
+    passes alone.  CUDA events on the current stream, after warm-up."""
+    import torch
+
+    from kwave import _lib
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = []
+    for nx, ny, nz in grids:
+        plan = _lib.Fft3d(nx, ny, nz)
+        x = torch.randn((nz, ny, nx), device="cuda", dtype=torch.float32)
+        spec = torch.zeros((nz, ny, plan.nxp), device="cuda", dtype=torch.complex64)
+        back = torch.empty_like(x)
+        st = torch.cuda.current_stream().cuda_stream
+        X = torch.fft.rfftn(x)
+        row = {"grid": [nx, ny, nz],
+               "cufft_r2c_ms": timed(lambda: torch.fft.rfftn(x)),
+               "cufft_c2r_ms": timed(lambda: torch.fft.irfftn(X, s=(nz, ny, nx), norm="forward")),
+               "own_r2c_ms": timed(lambda: plan.exec(x.data_ptr(), spec.data_ptr(), False, 7, st)),
+               "own_c2r_ms": timed(lambda: plan.exec(back.data_ptr(), spec.data_ptr(), True, 7, st))}
+        row["own_pass_ms"] = {name: timed(lambda b=bit: plan.exec(x.data_ptr(), spec.data_ptr(), False, b, st))
+                              for name, bit in (("x_r2c", 1), ("y", 2), ("z", 4))}
+        plan.check()
+        plan.close()
+        row["own_vs_cufft_r2c"] = row["cufft_r2c_ms"] / row["own_r2c_ms"]
+        row["own_vs_cufft_c2r"] = row["cufft_c2r_ms"] / row["own_c2r_ms"]
+        out.append(row)
+    return {"grids": out,
+            "note": "own = the solver's passes run bare (kw_fft3d; in the time loop they are fused with the "
+                    "physics); cufft = torch.fft.rfftn / irfftn (norm='forward', unnormalised inverse); "
+                    "own_vs_cufft > 1 means the own transform is faster"}
+
+
 def run_reference(args):
     """The reference arm: the reference algorithm on the host cores (the
     oracle port, numpy + scipy.fft on every host thread), the same workload,
@@ -440,6 +487,7 @@ def main():
     ap.add_argument("--batch-nt", type=int, default=500, help="time steps of each batched simulation")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests in the served sample (0: skip)")
     ap.add_argument("--no-tune", action="store_true", help="keep the built-in launch schedule (no kw_tune)")
+    ap.add_argument("--no-fft-sample", action="store_true", help="skip the comparison with cuFFT")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -546,6 +594,8 @@ def main():
                                           f"(numpy/scipy.fft, all host threads), {per:.2f} s/step, "
                                           f"{per * k:.1f} s timed"}
     if rank == 0 and world == 1 and not args.shape:
+        if not args.no_fft_sample:
+            line["fft_vs_cufft"] = fft_sample()
         if args.batch_sims > 0:
             line["batched"] = batched_sample(args.batch_sims, args.batch_nt)
         if args.serve_requests > 0:

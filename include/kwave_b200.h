@@ -347,6 +347,28 @@ void kw_wisdom_forget(void);
 int kw_session_schedule(const kw_session* s, kw_schedule* sched);
 
 /*
+ * A plain real-to-complex transform of a 2D / 3D grid (nz = 1: 2D) run by the
+ * solver's own FFT passes, standing where the reference calls MATLAB's
+ * fftn / ifftn on a real field (kspaceFirstOrder3D.m:790, 905-907).  The
+ * time loop does not use it (it fuses every pass with the physics); it lets
+ * the passes be timed beside a library FFT (cuFFT) and checked on their own.
+ *   d_real: nx*ny*nz floats, x fastest; d_spec: nz*ny*nxp complex floats
+ *   ([z][y][kx], kx in [0, nx/2], nxp = nx/2 + 1 rounded up to even).
+ * inverse = 0: d_spec = fftn(d_real) (half spectrum).  inverse = 1: d_real =
+ * nx*ny*nz * ifftn(d_spec), unnormalised, and d_spec is overwritten.
+ * `passes` selects the axes to run (bit 0: x, bit 1: y, bit 2: z; 7 = all),
+ * so each pass can be timed alone.  Work is only enqueued on `stream`;
+ * kw_fft3d_check reports a device-side wait that ran out.  The plan holds
+ * the twiddle tables (device memory) of the device current at creation.
+ */
+typedef struct kw_fft3d_plan kw_fft3d_plan;
+int kw_fft3d_create(uint64_t nx, uint64_t ny, uint64_t nz, kw_fft3d_plan** plan, kw_status* status);
+int kw_fft3d_exec(kw_fft3d_plan* plan, int inverse, unsigned passes, float* d_real, void* d_spec, void* stream,
+                  kw_status* status);
+int kw_fft3d_check(kw_fft3d_plan* plan, kw_status* status);
+void kw_fft3d_destroy(kw_fft3d_plan* plan);
+
+/*
  * No counterpart in the reference.
  *
  * The k-space staggered gradient of a 2D field, for callers that cannot
@@ -363,9 +385,11 @@ int kw_session_schedule(const kw_session* s, kw_schedule* sched);
  *
  * It allocates nothing: its intermediate spectra live in a fixed static
  * device array sized for edges up to KW_NOALLOC_MAX_EDGE (8 MiB per device);
- * larger grids are rejected with KW_ERR_INVALID_ARGUMENT.  The first call on
- * each device does a one-time set-up (looks up that array's address), so
- * make it before any stream capture.  The array is shared by all calls on a
+ * larger grids are rejected with KW_ERR_INVALID_ARGUMENT.  Every call looks
+ * up that array's address on the current device; the first call on a device
+ * may also load the library's device code there, so make it before any
+ * stream capture.  A stream of another device is rejected.  The array is
+ * shared by all calls on a
  * device: calls that overlap in time on one device race and must be
  * serialised by the caller.
  */

@@ -28,7 +28,7 @@ CU_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
             "-I" + INCLUDE, "-I" + CSRC]
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-I" + INCLUDE, "-I" + CSRC, "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["kernels.cu", "kernels_tma.cu", "solver.cu", "tuner.cu", "batch.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "kernels_tma.cu", "solver.cu", "tuner.cu", "batch.cu", "noalloc.cu", "fft3d.cu"]
 CXX_SOURCES = ["hdf5_lite.cpp", "io.cpp"]
 
 

@@ -71,7 +71,14 @@ class Batch {
     try {
       for (uint64_t k = 0; k < n; ++k) step();
     } catch (...) {
-      for (size_t i = 0; i < ss.size(); ++i) ss[i]->st = own[i];
+      // the steps already enqueued on the batch stream still write the
+      // members' buffers: each member's own stream waits for them before
+      // its next work (best effort; the original error is what is reported)
+      const bool marked = cudaEventRecord(ev1, bst) == cudaSuccess;
+      for (size_t i = 0; i < ss.size(); ++i) {
+        ss[i]->st = own[i];
+        if (!marked || cudaStreamWaitEvent(own[i], ev1, 0) != cudaSuccess) cudaStreamSynchronize(bst);
+      }
       throw;
     }
     bk(cudaEventRecord(ev1, bst), "cudaEventRecord");

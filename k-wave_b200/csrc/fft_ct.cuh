@@ -151,6 +151,39 @@ __device__ __forceinline__ void ct_stage_io(const float2* __restrict__ tw, int l
   }
 }
 
+// The first stage with a caller-supplied loader: ld(l, pos) returns input
+// element pos of line l from wherever the caller keeps it (the row kernels
+// build each packed line from two raw half-spectrum rows on the fly).  In
+// place like ct_stage: every input is loaded before the block barrier and
+// every output stored after it, so the inputs may alias the output buffer.
+template <int N, bool INV, class L, class LD>
+__device__ __forceinline__ void ct_stage0_ld(float2* buf, int l, int tid, L lay, LD ld) {
+  constexpr int R = ct_radix(N, 0);
+  constexpr int NR = N / R;
+  constexpr int T = Ct<N>::T;
+  constexpr int NB = (NR + T - 1) / T;
+  float2 v[NB][R];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = tid + i * T;
+    if (NR % T == 0 || j < NR) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = ld(l, j + r * NR);
+      dft<R, INV>(v[i]);  // first stage: no twiddles
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = tid + i * T;
+    if (NR % T == 0 || j < NR) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[lay(l, j * R + r)] = v[i][r];
+    }
+  }
+  __syncthreads();
+}
+
 template <int N, int STAGE, bool INV, class L>
 __device__ __forceinline__ void ct_stages(float2* buf, const float2* __restrict__ tw, int l, int tid, L lay) {
   if constexpr (STAGE < Ct<N>::S) {
@@ -239,6 +272,16 @@ __device__ __forceinline__ void ct_fft(float2* buf, const float2* __restrict__ t
     tid = threadIdx.x - l * T;
   }
   ct_stages<N, 0, INV>(buf, tw, l, tid, lay);
+}
+
+// Row tiles (consecutive threads on consecutive butterflies of a line): the
+// first stage reads its inputs through `ld`, the others run in place.
+template <int N, bool INV, class L, class LD>
+__device__ __forceinline__ void ct_fft_rows_ld(float2* buf, const float2* __restrict__ tw, L lay, LD ld) {
+  constexpr int T = Ct<N>::T;
+  const int l = threadIdx.x / T, tid = threadIdx.x - l * T;
+  ct_stage0_ld<N, INV>(buf, l, tid, lay, ld);
+  ct_stages<N, 1, INV>(buf, tw, l, tid, lay);
 }
 
 }  // namespace kwb

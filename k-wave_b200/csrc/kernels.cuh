@@ -105,6 +105,14 @@ struct Sensor {
   float* min_all;
 };
 
+// Bounded waits of the row kernels (the mbarrier waits on their bulk
+// copies): time limit (0: the 2 s default) and the word a wait that runs
+// out writes its error code to.
+struct WaitCtl {
+  int* err;
+  unsigned long long limit_ns;
+};
+
 // ---------------------------------------------------------------------------
 // kernel argument blocks
 // ---------------------------------------------------------------------------
@@ -145,6 +153,7 @@ struct UArgs {
   DenseSource dsrc[3];
   Sensor sens[3];
   Clock clk;
+  WaitCtl wait;
 };
 
 struct RhoArgs {
@@ -168,6 +177,7 @@ struct RhoArgs {
   Sensor sens;
   Clock clk;
   const float2* S_rr;  // axisymmetric: the u_r / r spectrum, added to S[1] as it is read
+  WaitCtl wait;
 };
 
 struct EosArgs {
@@ -179,6 +189,7 @@ struct EosArgs {
   float2* S_p;
   Sensor sens;
   Clock clk;
+  WaitCtl wait;
 };
 
 }  // namespace kwb

@@ -22,6 +22,7 @@
 #include "fft_ct.cuh"
 #include "kernels.cuh"
 #include "spec_ops.cuh"
+#include "tma.cuh"
 
 namespace kwb {
 
@@ -66,7 +67,7 @@ __device__ __forceinline__ float2* tile_fft(float2* a, float2* b, const float2* 
 template <int NC, bool INV>
 __global__ void __launch_bounds__(Tile<NC>::THREADS) k_col_fft(ColArgs a, const __grid_constant__ FFTPlan plan,
                                                                const float2* __restrict__ tw_g) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   constexpr bool CT = NC > 0;
   const int n = CT ? NC : plan.n;
   const int tl = CT ? Tile<NC>::LINES : a.tl;
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(Tile<NC>::THREADS) k_fused_last(const __grid_c
                                                                   const __grid_constant__ FFTPlan plan,
                                                                   const float2* __restrict__ tw_g,
                                                                   const __grid_constant__ SpecTables T, int dim) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   constexpr bool CT = NC > 0;
   const int n = CT ? NC : plan.n;
   const int tl = CT ? Tile<NC>::LINES : a.tl;
@@ -457,6 +458,92 @@ struct TilePrefetch {
 };
 
 // ---------------------------------------------------------------------------
+// Bulk-copied spectrum rows.  A row tile's input half spectra are fetched by
+// cp.async.bulk straight into the tile's own transform buffer, raw (tile row
+// r at r * nxp), every field of the tile requested when the block starts, so
+// the loads overlap one another and the first transform instead of
+// stalling each phase.  The first inverse stage then builds each packed line
+// (rows 2l and 2l + 1 as real and imaginary parts) from the raw rows as it
+// reads them (RawRows), in place: all its inputs are read before the block
+// barrier that precedes its stores.
+// Needs: NC % 4 == 0 (an even pitch nxp = nx / 2 + 2, so rows are 16-byte
+// multiples), 2 nxp <= the packed line stride (the raw rows fit the buffer),
+// and buffers at 16-byte boundaries (an even lines x stride product).
+// ---------------------------------------------------------------------------
+template <int NC>
+struct RowBulk {
+  static constexpr int LS = NC + NC / 16 + 1;  // row_layout_stride(NC)
+  static constexpr bool OK = NC > 0 && NC % 4 == 0 && 2 * (NC / 2 + 2) <= LS &&
+                             (RTile<NC>::LINES * LS) % 2 == 0 && NC % 2 == 0;
+};
+
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Issued by warp 0: `rows` spectrum rows from row r0 into raw, completion on bar.
+__device__ __forceinline__ void bulk_rows(float2* raw, const float2* S, const Dims& d, long long r0, int rows,
+                                          uint64_t* bar) {
+  const unsigned bytes = (unsigned)d.nxp * 8u;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) mbar_expect_tx(bar, bytes * (unsigned)rows);
+  __syncwarp();
+  for (int r = lane; r < rows; r += 32) bulk_load_1d(raw + (long long)r * d.nxp, S + (r0 + r) * d.nxp, bytes, bar);
+}
+
+__device__ __forceinline__ int tile_rows(const Dims& d, long long r0, int L) {
+  return (int)min(2LL * L, d.row1 - r0);
+}
+
+__device__ __forceinline__ uint64_t wait_limit(const WaitCtl& w) { return w.limit_ns ? w.limit_ns : kWaitNs; }
+
+// Wait for one field's rows; false (for every thread) if any thread's wait ran out.
+__device__ __forceinline__ bool rows_ready(uint64_t* bar, const WaitCtl& w) {
+  const bool ok = mbar_wait(bar, 0, w.err, wait_limit(w));
+  return !__syncthreads_or(!ok);
+}
+
+// After a failed wait: thread 0 waits (bounded) for the copies still in
+// flight, so they land before the block's shared memory is released.
+__device__ __forceinline__ void drain_rows(uint64_t* bars, int from, int to, const WaitCtl& w) {
+  if (threadIdx.x == 0)
+    for (int f = from; f < to; ++f) mbar_wait(&bars[f], 0, nullptr, wait_limit(w));
+}
+
+// Element n of packed line l, read from raw rows 2l and 2l + 1: the full
+// spectrum of row 2l plus i times that of row 2l + 1, each from its half
+// spectrum (Hermitian), with the imaginary parts of the k = 0 and Nyquist
+// bins dropped, as load_c2r builds it.  `kmul` (optional) multiplies bin k.
+template <int NC>
+struct RawRows {
+  const float2* raw;
+  int nxp;
+  int rows;
+  const float2* kmul;
+  __device__ __forceinline__ float2 operator()(int l, int n) const {
+    const bool lo = 2 * n <= NC;
+    const int k = lo ? n : NC - n;
+    const int ra = 2 * l;
+    float2 A = make_float2(0.f, 0.f), B = A;
+    if (ra < rows) A = raw[ra * nxp + k];
+    if (ra + 1 < rows) B = raw[(ra + 1) * nxp + k];
+    if (kmul) {
+      const float2 m = __ldg(kmul + k);
+      A = c_mul(A, m);
+      B = c_mul(B, m);
+    }
+    if (k == 0 || 2 * k == NC) {
+      A.y = 0.f;
+      B.y = 0.f;
+    }
+    return lo ? make_float2(A.x - B.y, A.y + B.x) : make_float2(A.x + B.y, B.x - A.y);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // u update: C2R of the gradient, split-PML momentum update, velocity
 // sources, velocity sensors, R2C of the new velocity.  blockIdx.y = axis.
 // ---------------------------------------------------------------------------
@@ -464,7 +551,7 @@ template <int NC>
 __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
                                                            const __grid_constant__ FFTPlan plan,
                                                            const float2* __restrict__ tw_g, int Lrt) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   __shared__ int sh[2];
   constexpr bool CT = NC > 0;
   const int nx = CT ? NC : d.nx;
@@ -474,19 +561,44 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   float2* tw = sm;
   float2* B0 = sm + nx;
   float2* B1 = CT ? nullptr : B0 + L * lay.ls;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  __shared__ uint64_t rbar[1];
+  if constexpr (RowBulk<NC>::OK) {  // the tile's spectrum rows are requested first
+    if (threadIdx.x == 0) {
+      mbar_init(&rbar[0], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) bulk_rows(B0, a.S[ax], d, r0, tile_rows(d, r0, L), &rbar[0]);
+  }
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
-  load_c2r<NC>(a.S[ax], B0, lay, d, r0, L, a.kmul[ax]);
-  __syncthreads();
-  if constexpr (NC > 0 && NC % 4 == 0) {  // the epilogue's inputs stream in during the FFT
-    TilePrefetch pf(d, r0, L);
-    if (!a.init) pf.field(a.u[ax]);
-    pf.field(a.rinv[ax].p);
-    pf.sensor(a.sens[ax], fi);
+  float2* G;
+  if constexpr (RowBulk<NC>::OK) {
+    {  // the epilogue's inputs stream in during the wait and the FFT
+      TilePrefetch pf(d, r0, L);
+      if (!a.init) pf.field(a.u[ax]);
+      pf.field(a.rinv[ax].p);
+      pf.sensor(a.sens[ax], fi);
+    }
+    if (!rows_ready(&rbar[0], a.wait)) {
+      drain_rows(rbar, 0, 1, a.wait);
+      return;
+    }
+    ct_fft_rows_ld<NC, true>(B0, tw, lay, RawRows<NC>{B0, d.nxp, tile_rows(d, r0, L), a.kmul[ax]});
+    G = B0;
+  } else {
+    load_c2r<NC>(a.S[ax], B0, lay, d, r0, L, a.kmul[ax]);
+    __syncthreads();
+    if constexpr (NC > 0 && NC % 4 == 0) {  // the epilogue's inputs stream in during the FFT
+      TilePrefetch pf(d, r0, L);
+      if (!a.init) pf.field(a.u[ax]);
+      pf.field(a.rinv[ax].p);
+      pf.sensor(a.sens[ax], fi);
+    }
+    G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
   }
-  float2* G = tile_fft<NC, true, false>(B0, B1, tw, plan, L, lay);
   float2* W = (G == B0) ? B1 : B0;
   float* u = a.u[ax];
   const float* pml = a.pml_sg[ax];
@@ -617,7 +729,7 @@ template <int NC, int DIM>
 __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   __shared__ int sh[2];
   constexpr bool CT = NC > 0;
   const int nx = CT ? NC : d.nx;
@@ -627,8 +739,25 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
   float2* tw = sm;
   float2* pool[4];
   for (int b = 0; b < 4; ++b) pool[b] = sm + nx + b * L * lay.ls;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  // every divergence component's spectrum rows are requested first (not on
+  // axisymmetric grids, whose u_r / r spectrum is summed in as S[1] is read)
+  __shared__ uint64_t rbar[3];
+  const bool bulk = RowBulk<NC>::OK && !a.S_rr;
+  if constexpr (RowBulk<NC>::OK) {
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) mbar_init(&rbar[f], 1);
+        fence_mbar_init();
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        const int rows = tile_rows(d, r0, L);
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) bulk_rows(pool[f], a.S[f], d, r0, rows, &rbar[f]);
+      }
+    }
+  }
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
   // inverse x transforms of the divergence components
@@ -637,12 +766,14 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
   if constexpr (CT) {
 #pragma unroll 1
     for (int f = 0; f < dim; ++f) {
-      load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L, nullptr, f == 1 ? a.S_rr : nullptr);
-      __syncthreads();
+      if (!bulk) {
+        load_c2r<NC>(a.S[f], pool[f], lay, d, r0, L, nullptr, f == 1 ? a.S_rr : nullptr);
+        __syncthreads();
+      }
       if constexpr (NC % 4 == 0) {  // what the next phase reads streams in during this FFT
         TilePrefetch pf(d, r0, L);
         if (f + 1 < dim) {
-          pf.spectrum(a.S[f + 1]);
+          if (!bulk) pf.spectrum(a.S[f + 1]);
         } else {
           _Pragma("unroll") for (int g = 0; g < dim; ++g) pf.field(a.rho[g]);
           pf.field(a.rho0.p);
@@ -650,6 +781,16 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
           if (a.nonlinear) pf.field(a.bona.p);
           if (a.eos == 2) pf.field(a.tau.p);
           if (a.eos != 1) pf.sensor(a.sens, fi);
+        }
+      }
+      if constexpr (RowBulk<NC>::OK) {
+        if (bulk) {
+          if (!rows_ready(&rbar[f], a.wait)) {
+            drain_rows(rbar, f, dim, a.wait);
+            return;
+          }
+          ct_fft_rows_ld<NC, true>(pool[f], tw, lay, RawRows<NC>{pool[f], d.nxp, tile_rows(d, r0, L), nullptr});
+          continue;
         }
       }
       tile_fft<NC, true, false>(pool[f], nullptr, tw, plan, L, lay);
@@ -869,7 +1010,7 @@ template <int NC>
 __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_constant__ EosArgs a, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   __shared__ int sh[2];
   constexpr bool CT = NC > 0;
   const int nx = CT ? NC : d.nx;
@@ -879,12 +1020,46 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
   float2* P0 = sm + nx;
   float2* P1 = P0 + L * lay.ls;
   float2* P2 = CT ? nullptr : P1 + L * lay.ls;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  __shared__ uint64_t rbar[2];
+  if constexpr (RowBulk<NC>::OK) {  // both spectra's rows are requested first
+    if (threadIdx.x == 0) {
+      mbar_init(&rbar[0], 1);
+      mbar_init(&rbar[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int rows = tile_rows(d, r0, L);
+      bulk_rows(P0, a.S_a, d, r0, rows, &rbar[0]);
+      bulk_rows(P1, a.S_b, d, r0, rows, &rbar[1]);
+    }
+  }
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const int fi = record_index(a.clk);
   float2 *RA, *RB, *Wk;
-  load_c2r<NC>(a.S_a, P0, lay, d, r0, L);
-  if constexpr (CT) {
+  if constexpr (RowBulk<NC>::OK) {
+    {  // the epilogue's inputs stream in during the waits and the FFTs
+      TilePrefetch pf(d, r0, L);
+      pf.field(a.p_loc);
+      pf.field(a.c2tau.p);
+      pf.field(a.c2eta.p);
+      pf.sensor(a.sens, fi);
+    }
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) {
+      if (!rows_ready(&rbar[f], a.wait)) {
+        drain_rows(rbar, f, 2, a.wait);
+        return;
+      }
+      float2* P = f ? P1 : P0;
+      ct_fft_rows_ld<NC, true>(P, tw, lay, RawRows<NC>{P, d.nxp, tile_rows(d, r0, L), nullptr});
+    }
+    RA = P0;
+    RB = P1;
+    Wk = nullptr;
+  } else if constexpr (CT) {
+    load_c2r<NC>(a.S_a, P0, lay, d, r0, L);
     load_c2r<NC>(a.S_b, P1, lay, d, r0, L);
     __syncthreads();
     if constexpr (NC % 4 == 0) {  // the epilogue's inputs stream in during the FFTs
@@ -900,6 +1075,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
     RB = P1;
     Wk = nullptr;
   } else {
+    load_c2r<NC>(a.S_a, P0, lay, d, r0, L);
     __syncthreads();
     RA = tile_fft<NC, true, false>(P0, P1, tw, plan, L, lay);
     float2* f1 = (RA == P0) ? P1 : P0;
@@ -965,7 +1141,7 @@ template <int NC>
 __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_r2c(const float* __restrict__ f, float2* S, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   constexpr bool CT = NC > 0;
   const int nx = CT ? NC : d.nx;
   const int L = row_lines<NC>(Lrt);
@@ -992,7 +1168,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_c2r(const float2* __re
                                                              int accumulate, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   constexpr bool CT = NC > 0;
   const int nx = CT ? NC : d.nx;
   const int L = row_lines<NC>(Lrt);

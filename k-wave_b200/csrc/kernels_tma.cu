@@ -82,11 +82,20 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
     const int o = r / a.ncx;
     tile_coords(a.yaxis, r - o * a.ncx, a.outer0 + o, TL, x, y, z);
   };
-  auto issue = [&](int t, int s) {
+  // thread 0's record of the stages with a load in flight (bit s) and the
+  // parity of each one's pending phase, for the drain after a failed wait
+  // (in shared memory: it costs no registers in the transform loop)
+  __shared__ unsigned inflight, parity_bits;
+  if (threadIdx.x == 0) inflight = parity_bits = 0;
+  auto issue = [&](int t, int j) {  // tile t, consumed at loop iteration j
+    const int s = j % ST;
     int f, x, y, z;
     coords(t, f, x, y, z);
     mbar_expect_tx(&bar[s], TTile<NC>::BYTES);
+    if (t == a.wait.skip_tile) return;  // test hook: announced, never issued
     tma_load_3d(bufs + s * E, &a.map[f], x, y, z, &bar[s]);
+    inflight |= 1u << s;
+    parity_bits = (parity_bits & ~(1u << s)) | ((unsigned)((j / ST) & 1) << s);
   };
   if (threadIdx.x == 0) {
     for (int f = 0; f < a.nfields; ++f) prefetch_tmap(&a.map[f]);
@@ -94,11 +103,17 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
     if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
   }
   const ColLayout lay{TL};
+  bool aborted = false;
   int it = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
     const int s = it % ST;
     float2* b = bufs + s * E;
-    mbar_wait(&bar[s], (it / ST) & 1, a.err);
+    const bool ok = mbar_wait(&bar[s], (it / ST) & 1, a.err, a.wait.limit_ns);
+    if (__syncthreads_or(!ok)) {  // every thread leaves together; nothing more is issued
+      aborted = true;
+      break;
+    }
+    if (threadIdx.x == 0) inflight &= ~(1u << s);
     ct_fft<NC, INV, true, TL>(b, tw, lay);
     fence_async_smem();
     __syncthreads();
@@ -110,11 +125,16 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
       const int t2 = t + 2 * gridDim.x;
       if (t2 < ntiles) {
         bulk_wait_read<ST - 2>();  // the store out of the stage being refilled has read it
-        issue(t2, (it + 2) % ST);
+        issue(t2, it + 2);
       }
     }
   }
-  if (threadIdx.x == 0) bulk_wait<0>();
+  if (threadIdx.x == 0) {
+    bulk_wait<0>();
+    if (aborted)  // the loads still in flight land before the block's shared memory is released
+      for (int s = 0; s < ST; ++s)
+        if (inflight & (1u << s)) mbar_wait(&bar[s], (parity_bits >> s) & 1, nullptr, a.wait.limit_ns);
+  }
 }
 
 // Operator classes of the fused kernel: one instantiation per class keeps
@@ -171,12 +191,18 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
     o = r / a.ncx;
     cx = r - o * a.ncx;
   };
-  auto issue = [&](int t, int s) {
+  __shared__ unsigned inflight, parity_bits;  // thread 0: as in k_col_tma
+  if (threadIdx.x == 0) inflight = parity_bits = 0;
+  auto issue = [&](int t, int j) {  // tile t, consumed at loop iteration j
+    const int s = j & 1;
     int g, cx, o, x, y, z;
     decode(t, g, cx, o);
     tile_coords(a.yaxis, cx, o, TL, x, y, z);
     mbar_expect_tx(&bar[s], TTile<NC>::BYTES);
+    if (t == a.wait.skip_tile) return;  // test hook: announced, never issued
     tma_load_3d(inb + s * E, &a.in[g], x, y, z, &bar[s]);
+    inflight |= 1u << s;
+    parity_bits = (parity_bits & ~(1u << s)) | ((unsigned)((j >> 1) & 1) << s);
   };
   if (threadIdx.x == 0) {
     if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
@@ -189,6 +215,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
   constexpr int TPL = TH / TL;  // threads per line
   constexpr int M = CtHandoff<NC>::M;
   static_assert(TPL == Ct<NC>::T, "one line per group of T threads");
+  bool aborted = false;
   int it = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -269,10 +296,15 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
     auto refill = [&]() {  // F is consumed: refill this input stage with the tile two ahead
       if (threadIdx.x == 0) {
         const int t2 = t + 2 * gridDim.x;
-        if (t2 < ntiles) issue(t2, s);
+        if (t2 < ntiles) issue(t2, it + 2);
       }
     };
-    mbar_wait(&bar[s], (it >> 1) & 1, a.err);
+    const bool ok = mbar_wait(&bar[s], (it >> 1) & 1, a.err, a.wait.limit_ns);
+    if (__syncthreads_or(!ok)) {  // every thread leaves together; nothing more is issued
+      aborted = true;
+      break;
+    }
+    if (threadIdx.x == 0) inflight &= ~(1u << s);
     if constexpr (MODE == 1) {
       float2 u[M];
       // forward first stage in place; last stage, operator and inverse first
@@ -306,6 +338,9 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
       }
     }
   }
+  if (threadIdx.x == 0 && aborted)  // the loads still in flight land before shared memory is released
+    for (int s = 0; s < 2; ++s)
+      if (inflight & (1u << s)) mbar_wait(&bar[s], (parity_bits >> s) & 1, nullptr, a.wait.limit_ns);
 }
 
 // ---------------------------------------------------------------------------

@@ -6,6 +6,15 @@
 
 namespace kwb {
 
+// Limit of every mbarrier wait, and a test hook: the load of tile
+// `skip_tile` (-1: none) is announced on its barrier but never issued, so
+// that tile's wait can only end by running out (the failure-detection test
+// uses it; sessions set it from KWAVE_B200_TEST_SKIP_TMA_TILE).
+struct TmaWaitArgs {
+  unsigned long long limit_ns;
+  int skip_tile;
+};
+
 struct ColTmaArgs {
   CUtensorMap map[4];  // one per field; box {LINES, N, 1} (y pass) or {LINES, 1, N} (last axis)
   int nfields;
@@ -14,6 +23,7 @@ struct ColTmaArgs {
   int outer0;   // first outer index
   int yaxis;    // 1: the transformed axis is the tensor's y dimension, 2: z
   int* err;
+  TmaWaitArgs wait;
 };
 
 struct FusedTmaArgs {
@@ -28,6 +38,7 @@ struct FusedTmaArgs {
   int nin, fanout, ncx, nouter, yaxis, dim;
   int ncols;  // valid kx columns (nx / 2 + 1)
   int* err;
+  TmaWaitArgs wait;
 };
 
 }  // namespace kwb

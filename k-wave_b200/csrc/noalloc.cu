@@ -13,10 +13,12 @@
 //
 // Where the memory comes from: the intermediate half spectra live in one
 // file-scope __device__ array of fixed size (g_scratch below, 8 MiB: two
-// spectra of the largest accepted grid, 1024 x 1024).  The first call on each
-// device looks up its address with cudaGetSymbolAddress (which may load this
-// module onto the device) and raises the kernel's shared-memory limit; make
-// that first call, e.g. on a small grid, before any stream capture begins.
+// spectra of the largest accepted grid, 1024 x 1024).  Every call looks up
+// its address on the current device with cudaGetSymbolAddress and raises the
+// kernel's shared-memory limit (cheap once the module is loaded, and never
+// stale: a device reset or a new primary context gives a new address).  The
+// first call on a device may load this module onto it, so make that first
+// call, e.g. on a small grid, before any stream capture begins.
 // Twiddle factors and operator values are generated inside the kernel, so
 // nothing is copied from the host either.
 //
@@ -31,7 +33,6 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
-#include <mutex>
 
 #include "fft_engine.cuh"
 #include "kwave_b200.h"
@@ -44,7 +45,6 @@ constexpr int MAX_EDGE = KW_NOALLOC_MAX_EDGE;
 constexpr int MAX_NXH = MAX_EDGE / 2 + 1;
 constexpr int TL = 8;           // kx columns per CTA in the y pass
 constexpr int THREADS = 256;
-constexpr int MAX_DEVICES = 64;
 // y pass: twiddles + three column tiles; x passes need far less
 constexpr size_t MAX_SMEM = sizeof(float2) * ((size_t)MAX_EDGE + 3ull * MAX_EDGE * TL);
 
@@ -208,9 +208,6 @@ bool on_device(const void* p, int dev) {
   return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
 
-std::mutex g_setup_mutex;
-float2* g_scratch_ptr[MAX_DEVICES] = {};
-
 }  // namespace
 
 extern "C" int kw_kspace_gradient_noalloc(const float* d_f, float* d_gx, float* d_gy, uint64_t nx, uint64_t ny,
@@ -236,23 +233,25 @@ extern "C" int kw_kspace_gradient_noalloc(const float* d_f, float* d_gx, float* 
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(status, KW_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= MAX_DEVICES) return fail(status, KW_ERR_UNSUPPORTED, "device %d out of range", dev);
   if (!on_device(d_f, dev) || !on_device(d_gx, dev) || (d_gy && !on_device(d_gy, dev)))
     return fail(status, KW_ERR_INVALID_ARGUMENT, "d_f, d_gx and d_gy must be memory of the current device %d", dev);
-
-  {  // set-up, once per device, with that device current
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_scratch);
-      if (e != cudaSuccess)
-        return fail(status, KW_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-      e = cudaFuncSetAttribute(k_grad2d_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_SMEM);
-      if (e != cudaSuccess)
-        return fail(status, KW_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-      g_scratch_ptr[dev] = (float2*)p;
-    }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (st) {  // work enqueued on another device's stream would read this device's scratch address there
+    int sdev = -1;
+    e = cudaStreamGetDevice(st, &sdev);
+    if (e != cudaSuccess) return fail(status, KW_ERR_INVALID_ARGUMENT, "stream: %s", cudaGetErrorString(e));
+    if (sdev != dev)
+      return fail(status, KW_ERR_INVALID_ARGUMENT, "the stream belongs to device %d, the current device is %d", sdev,
+                  dev);
   }
+
+  // the scratch array's address on the current device, looked up on every
+  // call, with that device current
+  void* scratch = nullptr;
+  e = cudaGetSymbolAddress(&scratch, g_scratch);
+  if (e != cudaSuccess) return fail(status, KW_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+  e = cudaFuncSetAttribute(k_grad2d_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_SMEM);
+  if (e != cudaSuccess) return fail(status, KW_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
 
   const int NX = (int)nx, NY = (int)ny;
   a.f = d_f;
@@ -262,14 +261,13 @@ extern "C" int kw_kspace_gradient_noalloc(const float* d_f, float* d_gx, float* 
   a.ny = NY;
   a.nxh = NX / 2 + 1;
   a.ngrad = d_gy ? 2 : 1;
-  a.S[0] = g_scratch_ptr[dev];
-  a.S[1] = g_scratch_ptr[dev] + (size_t)MAX_EDGE * MAX_NXH;
+  a.S[0] = (float2*)scratch;
+  a.S[1] = (float2*)scratch + (size_t)MAX_EDGE * MAX_NXH;
   a.kx_step = (float)(2.0 * M_PI / (NX * (double)dx));
   a.ky_step = (float)(2.0 * M_PI / (NY * (double)dy));
   a.half_cdt = 0.5f * c_ref * dt;
   a.inv_n = (float)(1.0 / ((double)NX * NY));
 
-  cudaStream_t st = (cudaStream_t)stream;
   const size_t row_smem = sizeof(float2) * (NX + 2 * row_layout_stride(NX));
   const size_t col_smem = sizeof(float2) * ((size_t)NY + 3ull * NY * TL);
   const unsigned row_pairs = (unsigned)((NY + 1) / 2);

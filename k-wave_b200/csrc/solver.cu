@@ -319,6 +319,68 @@ const kw_input* Session::expand_axisymmetric(const kw_input* in) {
   return &asx.in;
 }
 
+// A fingerprint of a simulation's input, stored with its checkpoints: every
+// scalar and flag, the length of every array, and up to 65536 evenly spaced
+// elements of each array (64-bit FNV-1a over their bytes).  It tells apart
+// checkpoints of different media, sources, sensors, grids or time steps
+// without reading whole arrays at session creation.
+namespace {
+struct Fnv {
+  uint64_t h = 1469598103934665603ull;
+  void bytes(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  }
+  template <class T>
+  void val(T v) { bytes(&v, sizeof(v)); }
+  template <class T>
+  void sampled(const T* a, uint64_t n) {
+    val(n);
+    if (!a || n == 0) {
+      val<uint64_t>(0);
+      return;
+    }
+    const uint64_t m = std::min<uint64_t>(n, 65536);
+    for (uint64_t i = 0; i < m; ++i) val(a[m == 1 ? 0 : (i * (n - 1)) / (m - 1)]);
+  }
+};
+}  // namespace
+
+static uint64_t input_fingerprint(const kw_input* in) {
+  Fnv f;
+  for (uint64_t v : {in->Nx, in->Ny, in->Nz, in->Nt, in->pml_x_size, in->pml_y_size, in->pml_z_size,
+                     in->nonlinear_flag, in->absorbing_flag, in->p0_source_flag, in->p_source_flag,
+                     in->p_source_mode, in->p_source_many, in->ux_source_flag, in->uy_source_flag,
+                     in->uz_source_flag, in->u_source_mode, in->u_source_many, in->sensor_mask_type,
+                     in->transducer_source_flag, in->axisymmetric_flag})
+    f.val(v);
+  for (float v : {in->dx, in->dy, in->dz, in->dt, in->c_ref, in->pml_x_alpha, in->pml_y_alpha, in->pml_z_alpha,
+                  in->alpha_power})
+    f.val(v);
+  for (const kw_field* k : {&in->c0, &in->rho0, &in->rho0_sgx, &in->rho0_sgy, &in->rho0_sgz, &in->BonA,
+                            &in->alpha_coeff})
+    f.sampled(k->data, k->data ? k->numel : 0);
+  const uint64_t npts = in->Nx * in->Ny * in->Nz;
+  f.sampled(in->p0_source_flag ? in->p0_source_input : nullptr, in->p0_source_flag ? npts : 0);
+  f.sampled(in->p_source_index, in->p_source_index_numel);
+  const uint64_t p_rows = in->p_source_many ? in->p_source_index_numel : 1;
+  f.sampled(in->p_source_input, in->p_source_input ? in->p_source_flag * p_rows : 0);
+  f.sampled(in->u_source_index, in->u_source_index_numel);
+  const uint64_t u_rows = in->u_source_many ? in->u_source_index_numel : 1;
+  f.sampled(in->ux_source_input, in->ux_source_input ? in->ux_source_flag * u_rows : 0);
+  f.sampled(in->uy_source_input, in->uy_source_input ? in->uy_source_flag * u_rows : 0);
+  f.sampled(in->uz_source_input, in->uz_source_input ? in->uz_source_flag * u_rows : 0);
+  f.sampled(in->sensor_mask_index, in->sensor_mask_index_numel);
+  f.sampled(in->sensor_mask_corners, in->sensor_mask_corners_numel);
+  f.sampled(in->transducer_source_input, in->transducer_source_input_numel);
+  f.sampled(in->delay_mask, in->delay_mask ? in->u_source_index_numel : 0);
+  f.sampled(in->transducer_source_apodization,
+            in->transducer_source_apodization ? in->u_source_index_numel : 0);
+  f.sampled(in->sensor_interp_index, in->sensor_interp_numel);
+  f.sampled(in->sensor_interp_weight, in->sensor_interp_numel);
+  return f.h;
+}
+
 void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   allow_ring_ = allow_ring;
   if (!in || !o) throw KwError(KW_ERR_INVALID_ARGUMENT, "input and options must not be NULL");
@@ -330,6 +392,7 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   p_rows0 = in->p_source_index_numel;
   u_rows0 = in->u_source_index_numel;
   in_user = in;
+  input_fp = input_fingerprint(in);
   if (in->axisymmetric_flag) in = expand_axisymmetric(in);
   if (in->Ny == 1) throw KwError(KW_ERR_UNSUPPORTED, "1D simulations are not supported (Ny must be > 1)");
   for (uint64_t n : {in->Nx, in->Ny, in->Nz}) {
@@ -563,6 +626,13 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
   // TMA-fed column passes for the compile-time lengths they support
   const char* no_tma = std::getenv("KWAVE_B200_NO_TMA");
   const bool tma_ok = !(no_tma && no_tma[0] == '1');
+  // the TMA kernels' wait limit (microseconds; default 2 s) and the failure-
+  // detection test's hook (a tile whose load is never issued)
+  if (const char* w = std::getenv("KWAVE_B200_TMA_WAIT_US")) {
+    const double us = std::atof(w);
+    if (us > 0) tma_wait.limit_ns = (unsigned long long)(us * 1e3);
+  }
+  if (const char* k = std::getenv("KWAVE_B200_TEST_SKIP_TMA_TILE")) tma_wait.skip_tile = std::atoi(k);
   // use_tma[1]: the y pass in 3D, the fused last-axis operator in 2D
   use_tma[1] = tma_ok && (d.dim == 3 ? tma_col_supported(d.ny) : tma_fused_supported(d.ny));
   use_tma[2] = tma_ok && d.dim == 3 && tma_fused_supported(d.nz);
@@ -794,6 +864,7 @@ void Session::col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs) 
     ca.outer0 = z0;
     ca.yaxis = 1;
     ca.err = (int*)err_buf.p;
+    ca.wait = tma_wait;
     ck(launch_col_tma(inv, d.ny, ca, twd[1], st), "col_tma");
   } else {
     ColArgs ca{};
@@ -841,6 +912,7 @@ void Session::fused_pass(const std::vector<int>& ins, const std::vector<int>& ou
     fa.dim = d.dim;
     fa.ncols = d.nxh;
     fa.err = (int*)err_buf.p;
+    fa.wait = tma_wait;
     ck(launch_fused_tma(ns[last], fa, twd[last], T, st), "fused_tma");
   } else {
     FusedArgs fa{};
@@ -1192,6 +1264,7 @@ UArgs Session::u_args(float2* const* S) {
   ua.do_r2c = 1;
   ua.src = usrc;
   ua.clk = clk;
+  ua.wait = row_wait();
   return ua;
 }
 
@@ -1306,6 +1379,7 @@ void Session::enqueue_step_body(uint64_t t) {
     ra.dsrc = pdense;
     ra.sens = row_sens_p();
     ra.clk = clk;
+    ra.wait = row_wait();
     ra.S_rr = axisym ? (const float2*)S_buf[4].p : nullptr;
     if (eos == 1) {
       ra.p_loc = (float*)ploc_buf.p;
@@ -1338,6 +1412,7 @@ void Session::enqueue_step_body(uint64_t t) {
       ea.S_p = S[0];
       ea.sens = row_sens_p();
       ea.clk = clk;
+      ea.wait = row_wait();
       for_slabs([&](int z0, int nzs) {
         col_pass(true, f12, z0, nzs);
         ck(launch_x_eos(ea, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_eos");
@@ -1441,9 +1516,9 @@ void Session::save_checkpoint(const std::string& path) {
     ck(cudaMemcpy(host.back().data(), b->p, b->bytes, cudaMemcpyDeviceToHost), "checkpoint d2h");
     w.dataset("/" + nb.first, h5::DType::F32, {(uint64_t)host.back().size()}, host.back().data());
   }
-  const uint64_t meta[5] = {t_done, (uint64_t)d.nx, (uint64_t)d.ny, (uint64_t)d.nz, Nt};
-  const char* names[5] = {"t_index", "Nx", "Ny", "Nz", "Nt"};
-  for (int i = 0; i < 5; ++i) w.dataset(std::string("/") + names[i], h5::DType::U64, {1}, &meta[i]);
+  const uint64_t meta[6] = {t_done, (uint64_t)d.nx, (uint64_t)d.ny, (uint64_t)d.nz, Nt, input_fp};
+  const char* names[6] = {"t_index", "Nx", "Ny", "Nz", "Nt", "input_fingerprint"};
+  for (int i = 0; i < 6; ++i) w.dataset(std::string("/") + names[i], h5::DType::U64, {1}, &meta[i]);
   w.root_attribute("created_by", kw_version());
   w.root_attribute("file_type", "checkpoint");
   w.root_attribute("major_version", "1");
@@ -1469,6 +1544,10 @@ void Session::restore_checkpoint(const std::string& path) {
     if (one("Nx") != (uint64_t)d.nx || one("Ny") != (uint64_t)d.ny || one("Nz") != (uint64_t)d.nz ||
         one("Nt") != Nt)
       throw KwError(KW_ERR_INVALID_ARGUMENT, "the checkpoint belongs to a different simulation");
+    if (!r.exists("/input_fingerprint") || one("input_fingerprint") != input_fp)
+      throw KwError(KW_ERR_INVALID_ARGUMENT,
+                    "the checkpoint belongs to a different simulation (its input fingerprint differs: medium, "
+                    "sources, sensor or time step)");
     const uint64_t t = one("t_index");
     if (t > Nt) throw KwError(KW_ERR_IO, "checkpoint time index beyond Nt");
     for (auto& nb : state_buffers()) {

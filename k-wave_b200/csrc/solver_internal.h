@@ -127,6 +127,7 @@ class Session {
   int slab = 1;  // z planes per chain slab
   Schedule sched_{};
   const kw_input* in_user = nullptr;  // the caller's input (before any axisymmetric expansion)
+  uint64_t input_fp = 0;              // fingerprint of that input, kept with checkpoints
   // slabs of a chain alternate between st and st2, forked and joined by
   // events, so one slab's row kernel can run beside another's y passes
   cudaStream_t st2 = nullptr;
@@ -175,6 +176,8 @@ class Session {
   // TMA tensor maps over the half-spectrum buffers (y pass / z pass)
   bool use_tma[3]{false, false, false};
   CUtensorMap map_y[5], map_z[5];  // [4]: the axisymmetric u_r / r spectrum
+  TmaWaitArgs tma_wait{2000000000ull, -1};  // wait limit (2 s) and the test hook of the TMA kernels
+  WaitCtl row_wait() const { return WaitCtl{(int*)err_buf.p, tma_wait.limit_ns}; }  // the row kernels' waits
   Clock clk{};
   // sources
   SparseSource psrc{}, usrc{};

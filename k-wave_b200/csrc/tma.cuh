@@ -1,10 +1,13 @@
 // Tensor-memory-accelerator (TMA) bulk copies and mbarrier waits (sm_100a
 // inline PTX) used by the persistent streaming kernels.
 //
-// Every wait is bounded: after kWaitNs of wall time a wait gives up, records
-// an error code in the kernel's error word and returns, so a copy that never
-// completes ends the kernel instead of hanging the GPU.  The host checks the
-// error word after each synchronisation.
+// Every wait is bounded: after a time limit (a kernel argument, 2 s by
+// default) a wait gives up, records an error code in the kernel's error word
+// and returns false.  The kernels then leave their tile loops together
+// (every thread learns of the failure at the next block barrier), wait
+// (bounded again) for the copies they still have in flight and return, so a
+// copy that never completes ends the kernel instead of hanging the GPU.  The
+// host checks the error word after each synchronisation.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -12,7 +15,7 @@
 
 namespace kwb {
 
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
+constexpr uint64_t kWaitNs = 2000000000ull;  // default limit of one wait: 2 s
 enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -40,8 +43,8 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Wait for the phase with the given parity to complete.  Bounded: gives up
-// after kWaitNs of wall time, records KERR_TMA_TIMEOUT and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// after limit_ns of wall time, records KERR_TMA_TIMEOUT and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint64_t limit_ns) {
   const uint32_t a = smem_u32(bar);
   uint64_t t0 = 0;
   for (unsigned i = 0;; ++i) {
@@ -58,7 +61,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
       const uint64_t now = global_ns();
       if (t0 == 0)
         t0 = now;
-      else if (now - t0 > kWaitNs)
+      else if (now - t0 > limit_ns)
         break;
     }
   }

@@ -111,6 +111,7 @@ EXPORTED = [
     "kw_batch_create", "kw_batch_advance", "kw_batch_elapsed_ms", "kw_batch_sync", "kw_batch_graph_launches",
     "kw_batch_destroy",
     "kw_kspace_gradient_noalloc",
+    "kw_fft3d_create", "kw_fft3d_exec", "kw_fft3d_check", "kw_fft3d_destroy",
 ]
 
 
@@ -162,6 +163,12 @@ def _load():
     lib.kw_kspace_gradient_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                                                C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p,
                                                C.POINTER(KwStatus)]
+    lib.kw_fft3d_create.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(C.c_void_p), C.POINTER(KwStatus)]
+    lib.kw_fft3d_exec.argtypes = [C.c_void_p, C.c_int, C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(KwStatus)]
+    lib.kw_fft3d_check.argtypes = [C.c_void_p, C.POINTER(KwStatus)]
+    lib.kw_fft3d_destroy.argtypes = [C.c_void_p]
+    lib.kw_fft3d_destroy.restype = None
     return lib
 
 
@@ -574,6 +581,37 @@ def kspace_gradient_noalloc(d_f, d_gx, d_gy, nx, ny, dx, dy, c_ref, dt, stream=N
     st = KwStatus()
     _check(lib.kw_kspace_gradient_noalloc(d_f, d_gx, d_gy, int(nx), int(ny), float(dx), float(dy), float(c_ref),
                                           float(dt), stream, C.byref(st)), st)
+
+
+class Fft3d:
+    """kw_fft3d_*: the solver's own FFT passes as a plain real-to-complex
+    transform of an nx x ny x nz grid (nz = 1: 2D), on device buffers given
+    as integer pointers.  Spectrum layout [nz][ny][nxp] complex64 with
+    nxp = nx // 2 + 1 rounded up to even; the inverse is unnormalised."""
+
+    def __init__(self, nx, ny, nz=1):
+        self.shape = (int(nx), int(ny), int(nz))
+        self.nxp = (int(nx) // 2 + 2) // 2 * 2
+        h = C.c_void_p()
+        st = KwStatus()
+        _check(lib.kw_fft3d_create(int(nx), int(ny), int(nz), C.byref(h), C.byref(st)), st)
+        self._h = h
+
+    def exec(self, d_real, d_spec, inverse=False, passes=7, stream=None):
+        st = KwStatus()
+        _check(lib.kw_fft3d_exec(self._h, int(bool(inverse)), int(passes), d_real, d_spec, stream, C.byref(st)), st)
+
+    def check(self):
+        st = KwStatus()
+        _check(lib.kw_fft3d_check(self._h, C.byref(st)), st)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.kw_fft3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def version():

@@ -15,7 +15,7 @@ HEADER = os.path.join(ROOT, "include", "kwave_b200.h")
 
 def declared_functions():
     src = open(HEADER).read()
-    decl = r"^(?:int|void|void\s*\*|const char\s*\*|uint64_t)\s*\**\s*(kw_[a-z_]+)\s*\("
+    decl = r"^(?:int|void|void\s*\*|const char\s*\*|uint64_t)\s*\**\s*(kw_[a-z0-9_]+)\s*\("
     return sorted(set(re.findall(decl, src, re.M)))
 
 
