@@ -368,7 +368,47 @@ __device__ __forceinline__ float2 kahan_add(float2 acc, float v) {
   return acc;
 }
 
-// Dense sensors and full-grid reductions for 4 consecutive points.
+// Dense sensors and full-grid reductions for 4 consecutive points, split
+// into a load and a store part so that an epilogue issues every load of an
+// iteration (its own inputs and the accumulators) before any store: a store
+// through another pointer (p, say) would otherwise keep the accumulator loads
+// behind it, a second memory round trip per iteration.
+struct Acc4 {  // the accumulators loaded ahead: per-point max and the Kahan rms pair
+  float4 mx, r0, r1;
+};
+__device__ __forceinline__ void sensor_dense4_load(const Sensor& s, int fi, long long gi, Acc4& c) {
+  if (fi <= 1 || s.mode != 1) return;  // fi 1: the accumulators start here; <= 0: nothing recorded yet
+  if (s.vmax) c.mx = ld4(s.vmax, gi);
+  if (s.rms) {
+    const float4* r = reinterpret_cast<const float4*>(s.rms + gi);
+    c.r0 = r[0];
+    c.r1 = r[1];
+  }
+}
+// (the less common accumulators -- per-point min, full-grid max / min -- are
+// loaded here, where they are updated)
+__device__ __forceinline__ void sensor_dense4_store(const Sensor& s, int fi, long long gi, float4 v, const Acc4& c) {
+  if (fi <= 0) return;
+  if (s.mode == 1) {
+    if (s.raw) st4(s.raw, raw_row(s, fi) * s.ns + gi, v);
+    if (s.vmax) st4(s.vmax, gi, fi == 1 ? v : max4(c.mx, v));
+    if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
+    if (s.rms) {
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 a = (fi == 1) ? z : c.r0, b = (fi == 1) ? z : c.r1;
+      float2 t0 = kahan_add(make_float2(a.x, a.y), v.x), t1 = kahan_add(make_float2(a.z, a.w), v.y);
+      float2 t2 = kahan_add(make_float2(b.x, b.y), v.z), t3 = kahan_add(make_float2(b.z, b.w), v.w);
+      float4* r = reinterpret_cast<float4*>(s.rms + gi);
+      r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
+      r[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+    }
+  }
+  if (s.max_all) st4(s.max_all, gi, fi == 1 ? v : max4(ld4(s.max_all, gi), v));
+  if (s.min_all) st4(s.min_all, gi, fi == 1 ? v : min4(ld4(s.min_all, gi), v));
+}
+
+// Both parts at once, each accumulator loaded where it is updated (fewer
+// live registers; used where the loads need not run ahead of a store).
 __device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long gi, float4 v) {
   if (fi <= 0) return;
   if (s.mode == 1) {
@@ -377,8 +417,8 @@ __device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long
     if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
     if (s.rms) {
       float4* r = reinterpret_cast<float4*>(s.rms + gi);
-      float4 a = (fi == 1) ? make_float4(0.f, 0.f, 0.f, 0.f) : r[0];
-      float4 b = (fi == 1) ? make_float4(0.f, 0.f, 0.f, 0.f) : r[1];
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 a = (fi == 1) ? z : r[0], b = (fi == 1) ? z : r[1];
       float2 t0 = kahan_add(make_float2(a.x, a.y), v.x), t1 = kahan_add(make_float2(a.z, a.w), v.y);
       float2 t2 = kahan_add(make_float2(b.x, b.y), v.z), t3 = kahan_add(make_float2(b.z, b.w), v.w);
       r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
@@ -855,6 +895,8 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       const float4 ta4 = (a.eos == 2) ? map4(a.tau, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 ds4 = dense_on ? __ldg(reinterpret_cast<const float4*>(a.dsrc.field + gi))
                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+      Acc4 acc;  // the sensor accumulators (lossless / Stokes), loaded before any store
+      if (!absorbing) sensor_dense4_load(a.sens, fi, gi, acc);
       float rn[3][4], outp[4], outq[4], outr[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -902,7 +944,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
         st4(a.p_loc, gi, pv4);
       } else {
         if (a.p_out) st4(a.p_out, gi, pv4);
-        sensor_dense4(a.sens, fi, gi, pv4);
+        sensor_dense4_store(a.sens, fi, gi, pv4, acc);
       }
     }
   } else {
@@ -1086,28 +1128,52 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
   }
   const int total = 2 * L * nx;
   if constexpr (NC > 0 && NC % 4 == 0) {
-#pragma unroll (kRowLoopUnroll)
-    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
-      const int q = i / nx, x = i - q * nx;
-      const long long row = r0 + q;
-      if (row >= d.row1) {
+    // 4 points per iteration: every load (inputs and sensor accumulators)
+    // is issued before any store
+    struct In {
+      float4 pl, ct, ce;
+      Acc4 acc;
+      long long gi;
+      int q, x;
+      bool ok;
+    };
+    auto load = [&](int i, In& v) {
+      v.q = i / nx;
+      v.x = i - v.q * nx;
+      const long long row = r0 + v.q;
+      v.ok = row < d.row1;
+      if (!v.ok) return;
+      v.gi = row * nx + v.x;
+      v.pl = ld4(a.p_loc, v.gi);
+      v.ct = map4(a.c2tau, v.gi);
+      v.ce = map4(a.c2eta, v.gi);
+      sensor_dense4_load(a.sens, fi, v.gi, v.acc);
+    };
+    auto update = [&](const In& v) {
+      if (!v.ok) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) set_comp(RA, lay, q, x + j, 0.f);
-        continue;
+        for (int j = 0; j < 4; ++j) set_comp(RA, lay, v.q, v.x + j, 0.f);
+        return;
       }
-      const long long gi = row * nx + x;
-      const float4 pl = ld4(a.p_loc, gi), ct = map4(a.c2tau, gi), ce = map4(a.c2eta, gi);
-      const float plv[4] = {pl.x, pl.y, pl.z, pl.w}, ctv[4] = {ct.x, ct.y, ct.z, ct.w};
-      const float cev[4] = {ce.x, ce.y, ce.z, ce.w};
+      const float plv[4] = {v.pl.x, v.pl.y, v.pl.z, v.pl.w}, ctv[4] = {v.ct.x, v.ct.y, v.ct.z, v.ct.w};
+      const float cev[4] = {v.ce.x, v.ce.y, v.ce.z, v.ce.w};
       float pv[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        pv[j] = plv[j] + ctv[j] * get_comp(RA, lay, q, x + j) - cev[j] * get_comp(RB, lay, q, x + j);
-        set_comp(RA, lay, q, x + j, pv[j]);
+        pv[j] = plv[j] + ctv[j] * get_comp(RA, lay, v.q, v.x + j) - cev[j] * get_comp(RB, lay, v.q, v.x + j);
+        set_comp(RA, lay, v.q, v.x + j, pv[j]);
       }
       const float4 p4 = make_float4(pv[0], pv[1], pv[2], pv[3]);
-      if (a.p_out) st4(a.p_out, gi, p4);
-      sensor_dense4(a.sens, fi, gi, p4);
+      if (a.p_out) st4(a.p_out, v.gi, p4);
+      sensor_dense4_store(a.sens, fi, v.gi, p4, v.acc);
+    };
+    // (issuing two iterations' loads together measured the same: 1.2622
+    // against 1.2616 ms per 256^3 step, at 113 instead of 72 registers)
+#pragma unroll 1
+    for (int i = 4 * threadIdx.x; i < total; i += 4 * blockDim.x) {
+      In v;
+      load(i, v);
+      update(v);
     }
   } else {
 #pragma unroll 4
