@@ -602,16 +602,20 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   float2* B0 = sm + nx;
   float2* B1 = CT ? nullptr : B0 + L * lay.ls;
   const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   __shared__ uint64_t rbar[1];
-  if constexpr (RowBulk<NC>::OK) {  // the tile's spectrum rows are requested first
+  if constexpr (RowBulk<NC>::OK) {
     if (threadIdx.x == 0) {
       mbar_init(&rbar[0], 1);
       fence_mbar_init();
     }
+  }
+  pdl_wait();  // everything below reads or writes the predecessors' data
+  pdl_trigger();
+  if constexpr (RowBulk<NC>::OK) {  // the tile's spectrum rows are requested first
     __syncthreads();
     if (threadIdx.x < 32) bulk_rows(B0, a.S[ax], d, r0, tile_rows(d, r0, L), &rbar[0]);
   }
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
   float2* G;
@@ -780,16 +784,21 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
   float2* pool[4];
   for (int b = 0; b < 4; ++b) pool[b] = sm + nx + b * L * lay.ls;
   const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   // every divergence component's spectrum rows are requested first (not on
   // axisymmetric grids, whose u_r / r spectrum is summed in as S[1] is read)
   __shared__ uint64_t rbar[3];
   const bool bulk = RowBulk<NC>::OK && !a.S_rr;
   if constexpr (RowBulk<NC>::OK) {
+    if (bulk && threadIdx.x == 0) {
+      _Pragma("unroll") for (int f = 0; f < dim; ++f) mbar_init(&rbar[f], 1);
+      fence_mbar_init();
+    }
+  }
+  pdl_wait();  // everything below reads or writes the predecessors' data
+  pdl_trigger();
+  if constexpr (RowBulk<NC>::OK) {
     if (bulk) {
-      if (threadIdx.x == 0) {
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) mbar_init(&rbar[f], 1);
-        fence_mbar_init();
-      }
       __syncthreads();
       if (threadIdx.x < 32) {
         const int rows = tile_rows(d, r0, L);
@@ -797,7 +806,6 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       }
     }
   }
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const int t = *a.clk.t;
   const int fi = record_index(a.clk);
   // inverse x transforms of the divergence components
@@ -1063,13 +1071,18 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
   float2* P1 = P0 + L * lay.ls;
   float2* P2 = CT ? nullptr : P1 + L * lay.ls;
   const long long r0 = d.row0 + (long long)blockIdx.x * 2 * L;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   __shared__ uint64_t rbar[2];
-  if constexpr (RowBulk<NC>::OK) {  // both spectra's rows are requested first
+  if constexpr (RowBulk<NC>::OK) {
     if (threadIdx.x == 0) {
       mbar_init(&rbar[0], 1);
       mbar_init(&rbar[1], 1);
       fence_mbar_init();
     }
+  }
+  pdl_wait();  // everything below reads or writes the predecessors' data
+  pdl_trigger();
+  if constexpr (RowBulk<NC>::OK) {  // both spectra's rows are requested first
     __syncthreads();
     if (threadIdx.x < 32) {
       const int rows = tile_rows(d, r0, L);
@@ -1077,7 +1090,6 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_eos(const __grid_const
       bulk_rows(P1, a.S_b, d, r0, rows, &rbar[1]);
     }
   }
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = tw_g[i];
   const int fi = record_index(a.clk);
   float2 *RA, *RB, *Wk;
   if constexpr (RowBulk<NC>::OK) {
@@ -1306,7 +1318,7 @@ static void x_u_t(const UArgs& a, const Dims& d, const FFTPlan& plan, const floa
   const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
   set_smem(k_x_u<NC>, sm);
-  k_x_u<NC><<<dim3(row_tiles(d, L), d.dim), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  launch_pdl(k_x_u<NC>, dim3(row_tiles(d, L), d.dim), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
 }
 
 template <int NC>
@@ -1316,10 +1328,10 @@ static void x_rho_t(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const 
   const size_t sm = smem_row(d.nx, L, NC > 0 ? d.dim : d.dim + 1);
   if (d.dim == 3) {
     set_smem(k_x_rho<NC, 3>, sm);
-    k_x_rho<NC, 3><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+    launch_pdl(k_x_rho<NC, 3>, dim3(row_tiles(d, L)), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
   } else {
     set_smem(k_x_rho<NC, 2>, sm);
-    k_x_rho<NC, 2><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+    launch_pdl(k_x_rho<NC, 2>, dim3(row_tiles(d, L)), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
   }
 }
 
@@ -1329,7 +1341,7 @@ static void x_eos_t(const EosArgs& a, const Dims& d, const FFTPlan& plan, const 
   const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 2 : 3);
   set_smem(k_x_eos<NC>, sm);
-  k_x_eos<NC><<<row_tiles(d, L), RTile<NC>::THREADS, sm, st>>>(a, d, plan, tw, L);
+  launch_pdl(k_x_eos<NC>, dim3(row_tiles(d, L)), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
 }
 
 template <int NC>

@@ -97,8 +97,11 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
     inflight |= 1u << s;
     parity_bits = (parity_bits & ~(1u << s)) | ((unsigned)((j / ST) & 1) << s);
   };
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0)
     for (int f = 0; f < a.nfields; ++f) prefetch_tmap(&a.map[f]);
+  pdl_wait();  // the fields are the predecessors' outputs
+  pdl_trigger();
+  if (threadIdx.x == 0) {
     if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
     if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
   }
@@ -183,13 +186,21 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
     }
   }
   __syncthreads();
-  const int per_in = a.ncx * a.nouter;
+  const int main_in = a.ncx * a.nouter;  // column tiles of one input
+  const int per_in = main_in + a.nrem;
   const int ntiles = a.nin * per_in;
+  // tile t -> input g and, for a column tile, its first column cx and outer
+  // index o; a remainder tile has cx = -1 and its first outer index in o
   auto decode = [&](int t, int& g, int& cx, int& o) {
     g = t / per_in;
     const int r = t - g * per_in;
-    o = r / a.ncx;
-    cx = r - o * a.ncx;
+    if (r < main_in) {
+      o = r / a.ncx;
+      cx = r - o * a.ncx;
+    } else {
+      cx = -1;
+      o = (r - main_in) * a.rem_y;
+    }
   };
   __shared__ unsigned inflight, parity_bits;  // thread 0: as in k_col_tma
   if (threadIdx.x == 0) inflight = parity_bits = 0;
@@ -197,13 +208,19 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
     const int s = j & 1;
     int g, cx, o, x, y, z;
     decode(t, g, cx, o);
-    tile_coords(a.yaxis, cx, o, TL, x, y, z);
-    mbar_expect_tx(&bar[s], TTile<NC>::BYTES);
+    mbar_expect_tx(&bar[s], TTile<NC>::BYTES);  // a remainder box holds as many bytes
     if (t == a.wait.skip_tile) return;  // test hook: announced, never issued
-    tma_load_3d(inb + s * E, &a.in[g], x, y, z, &bar[s]);
+    if (cx >= 0) {
+      tile_coords(a.yaxis, cx, o, TL, x, y, z);
+      tma_load_3d(inb + s * E, &a.in[g], x, y, z, &bar[s]);
+    } else {
+      tma_load_3d(inb + s * E, &a.in_rem[g], a.ncols - 1, o, 0, &bar[s]);
+    }
     inflight |= 1u << s;
     parity_bits = (parity_bits & ~(1u << s)) | ((unsigned)((j >> 1) & 1) << s);
   };
+  pdl_wait();  // the inputs are the predecessors' outputs
+  pdl_trigger();
   if (threadIdx.x == 0) {
     if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
     if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
@@ -222,9 +239,24 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
     float2* F = inb + s * E;
     int g, cx, o;
     decode(t, g, cx, o);
-    const int x0 = cx * TL;
-    const int ix = min(x0 + l, a.ncols - 1);
-    const float kxy2 = __ldg(T.k2[0] + ix) + ((a.dim == 3) ? __ldg(T.k2[1] + o) : 0.f);
+    // this thread's line: its column ix and outer index ol, where its
+    // output goes (loff) and whether it is a real column (valid)
+    int ix, ol;
+    long long loff;
+    bool valid;
+    if (cx >= 0) {
+      const int x0 = cx * TL;
+      ix = min(x0 + l, a.ncols - 1);
+      ol = o;
+      loff = (long long)o * a.ostride + x0 + l;
+      valid = (x0 + l) < a.ncols;
+    } else {  // lines alternate the last column and the padding bin
+      ix = a.ncols - 1;
+      ol = o + (l >> 1);
+      loff = (long long)ol * a.ostride + ix;
+      valid = (l & 1) == 0;
+    }
+    const float kxy2 = __ldg(T.k2[0] + ix) + ((a.dim == 3) ? __ldg(T.k2[1] + ol) : 0.f);
     // the operator of output q: a real factor m(|k|^2), times a complex
     // factor that is constant along the line or read from a line table
     struct OpEval {
@@ -245,7 +277,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
             const float2* tab = (op.kind == OP_GRAD_POS)   ? T.ddk_pos[op.axis]
                                 : (op.kind == OP_GRAD_NEG) ? T.ddk_neg[op.axis]
                                                            : T.shift_neg[op.axis];  // shift, kappa * shift
-            ev.dconst = __ldg(tab + (op.axis == 0 ? ix : o));
+            ev.dconst = __ldg(tab + (op.axis == 0 ? ix : ol));
           }
         }
       } else if constexpr (CLS == FC_NABLA) {
@@ -274,19 +306,18 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
     // inverse last stage, straight from W to the output (and the optional
     // second output scaled by a factor constant along the line)
     auto finish = [&](int q, const float2* src) {
-      float2* dst = a.outp[g * a.fanout + q] + (long long)o * a.ostride + x0;
+      float2* dst = a.outp[g * a.fanout + q] + loff;
       float2* dst2 = a.dual_outp[g * a.fanout + q];
       float2 dsc = make_float2(0.f, 0.f);
       if (dst2) {
-        dst2 += (long long)o * a.ostride + x0;
-        dsc = __ldg(a.dual_tab[g * a.fanout + q] + o);
+        dst2 += loff;
+        dsc = __ldg(a.dual_tab[g * a.fanout + q] + ol);
       }
-      const bool valid = (x0 + l) < a.ncols;
       auto ld_w = [&](int ll, int pos) -> float2 { return src[lay(ll, pos)]; };
-      auto st_g = [&](int ll, int pos, float2 v) {
+      auto st_g = [&](int, int pos, float2 v) {  // (the line is this thread's, folded into loff)
         if (valid) {
-          dst[pos * a.lstride + ll] = v;
-          if (dst2) dst2[pos * a.lstride + ll] = c_mul(v, dsc);
+          dst[pos * a.lstride] = v;
+          if (dst2) dst2[pos * a.lstride] = c_mul(v, dsc);
         }
       };
       ct_stage_io<NC, 1, true>(tw, l, tid, ld_w, st_g);
@@ -396,6 +427,22 @@ bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n) 
   return r == CUDA_SUCCESS;
 }
 
+// Tensor map of the remainder tiles of the last-axis pass (3D): box {2,
+// rows, nz} at x = nxh - 1, the lone last column and the bin past it (zero-
+// filled on load; its lines are not stored).
+bool make_spec_map_rem(CUtensorMap* m, void* base, const Dims& d, int n, int rows) {
+  if (!get_encoder()) return false;
+  if (d.nxp % 2 != 0 || (d.nxh - 1) % 2 != 0 || rows < 1 || rows > 256 || n > 256) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)d.nxh, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
+  cuuint64_t strides[2] = {(cuuint64_t)d.nxp * 8, (cuuint64_t)d.nxp * d.ny * 8};
+  cuuint32_t box[3] = {2u, (cuuint32_t)rows, (cuuint32_t)n};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 static int g_num_sms = 0;
 static int num_sms() {
   if (!g_num_sms) {
@@ -415,8 +462,8 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
   const int ntiles = a.nfields * a.ncx * a.nouter;
   const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
-  k<<<grid, TTile<NC>::THREADS, sm, st>>>(a, tw);
-  return cudaGetLastError();
+  const cudaError_t e = launch_pdl(k, dim3(grid), dim3(TTile<NC>::THREADS), sm, st, a, tw);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int NC, int CLS, int MODE>
@@ -427,10 +474,10 @@ static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const Sp
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
-  const int ntiles = a.nin * a.ncx * a.nouter;
+  const int ntiles = a.nin * (a.ncx * a.nouter + a.nrem);
   const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
-  k<<<grid, TTile<NC>::THREADS, sm, st>>>(a, tw, T);
-  return cudaGetLastError();
+  const cudaError_t e = launch_pdl(k, dim3(grid), dim3(TTile<NC>::THREADS), sm, st, a, tw, T);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int NC>

@@ -37,6 +37,13 @@ struct FusedTmaArgs {
   long long ostride;    // stride of the outer index
   int nin, fanout, ncx, nouter, yaxis, dim;
   int ncols;  // valid kx columns (nx / 2 + 1)
+  // Remainder tiles (3D): when the last column kx = ncols - 1 would be alone
+  // in its column tile, it is gathered for rem_y consecutive outer indices
+  // into one tile instead (box {2, rem_y, n}, lines alternating kx = ncols - 1
+  // and the zero-filled padding bin), so the ncx column tiles stop at
+  // ncols - 1.  nrem: remainder tiles per input (0: none).
+  CUtensorMap in_rem[3];
+  int nrem, rem_y;
   int* err;
   TmaWaitArgs wait;
 };

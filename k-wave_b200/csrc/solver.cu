@@ -66,6 +66,7 @@ bool tma_col_supported(int n);    // TMA-fed y pass
 bool tma_fused_supported(int n);  // TMA-fed fused last-axis operator
 int tma_lines(int n);
 bool make_spec_map(CUtensorMap* m, void* base, const Dims& d, int yaxis, int n);
+bool make_spec_map_rem(CUtensorMap* m, void* base, const Dims& d, int n, int rows);
 cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* tw, cudaStream_t st);
 cudaError_t launch_fused_tma(int n, const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st);
 
@@ -640,6 +641,15 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
     if (use_tma[1] && !make_spec_map(&map_y[s], S_buf[s].p, d, 1, d.ny)) use_tma[1] = false;
     if (use_tma[2] && !make_spec_map(&map_z[s], S_buf[s].p, d, 2, d.nz)) use_tma[2] = false;
   }
+  // last-axis remainder tiles: when kx = nx / 2 would be alone in its column
+  // tile, it is gathered for TL / 2 consecutive y into one tile instead
+  {
+    const int tl = use_tma[2] ? tma_lines(d.nz) : 0;
+    rem_y = tl / 2;
+    use_rem = use_tma[2] && tl % 2 == 0 && (d.nxh - 1) % tl == 0 && (d.nxh - 1) % 2 == 0 && d.ny % rem_y == 0;
+    for (int s = 0; s < nspec && use_rem; ++s)
+      if (!make_spec_map_rem(&map_zr[s], S_buf[s].p, d, d.nz, rem_y)) use_rem = false;
+  }
   if (eos == 1) ploc_buf.alloc(fb, st);
   if (opt.p_final) {
     p_buf.alloc(fb, st);
@@ -908,6 +918,12 @@ void Session::fused_pass(const std::vector<int>& ins, const std::vector<int>& ou
     fa.fanout = fanout;
     fa.ncx = (d.nxh + tma_lines(ns[last]) - 1) / tma_lines(ns[last]);
     fa.nouter = (d.dim == 3) ? d.ny : 1;
+    if (d.dim == 3 && use_rem) {
+      fa.ncx = (d.nxh - 1) / tma_lines(ns[last]);
+      fa.nrem = d.ny / rem_y;
+      fa.rem_y = rem_y;
+      for (int i = 0; i < nin; ++i) fa.in_rem[i] = map_zr[ins[i]];
+    }
     fa.yaxis = (d.dim == 3) ? 2 : 1;
     fa.dim = d.dim;
     fa.ncols = d.nxh;
@@ -957,6 +973,12 @@ void Session::grad_pass() {
     fused_pass({0}, {1, 2}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 1}}, 2);
 }
 
+// The y-inverse / row kernel / y-forward chain over z slabs; with two
+// streams the slabs alternate between them and all start together.
+// (Starting each slab after the previous slab's y-inverse pass, so that a
+// y pass runs beside the other slab's row kernel, measured slower: 1.316
+// against 1.260 ms per 256^3 step with two slabs, 1.308 against 1.282 with
+// four.)
 template <class F>
 void Session::for_slabs(F&& body) {
   if (!st2) {

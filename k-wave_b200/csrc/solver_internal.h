@@ -176,6 +176,9 @@ class Session {
   // TMA tensor maps over the half-spectrum buffers (y pass / z pass)
   bool use_tma[3]{false, false, false};
   CUtensorMap map_y[5], map_z[5];  // [4]: the axisymmetric u_r / r spectrum
+  CUtensorMap map_zr[5];           // last-axis remainder tiles (box {2, rem_y, nz})
+  bool use_rem = false;
+  int rem_y = 0;
   TmaWaitArgs tma_wait{2000000000ull, -1};  // wait limit (2 s) and the test hook of the TMA kernels
   WaitCtl row_wait() const { return WaitCtl{(int*)err_buf.p, tma_wait.limit_ns}; }  // the row kernels' waits
   Clock clk{};

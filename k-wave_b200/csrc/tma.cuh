@@ -109,4 +109,35 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// Programmatic dependent launch.  The step's kernels are launched with
+// programmatic stream serialization (launch_pdl): a kernel may become
+// resident while its predecessor in the stream finishes, runs the set-up that
+// reads nothing the predecessor writes (barrier initialisation, twiddle and
+// operator tables, tensor-map prefetch), and then waits in pdl_wait() until
+// the predecessor has completed and its memory is visible.  Every global
+// access that depends on earlier kernels -- reads and writes -- comes after
+// pdl_wait().  pdl_trigger() lets the successor launch; it is issued after
+// the wait, so at most one kernel ahead waits for resources.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Host: launch with programmatic stream serialization (off with
+// KWAVE_B200_NO_PDL=1).
+bool pdl_enabled();
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 }  // namespace kwb
