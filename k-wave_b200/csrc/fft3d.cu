@@ -79,6 +79,7 @@ void column_pass(const kw_fft3d_plan& p, int axis, bool inv, float2* S, cudaStre
     std::memset(&ca, 0, sizeof(ca));
     if (!make_spec_map(&ca.map[0], S, d, axis, n)) throw std::runtime_error("tensor map of the spectrum");
     ca.nfields = 1;
+    ca.dual_field = ca.dual_src = -1;
     ca.ncx = (d.nxh + tma_lines(n) - 1) / tma_lines(n);
     ca.nouter = axis == 1 ? d.nz : d.ny;
     ca.outer0 = 0;

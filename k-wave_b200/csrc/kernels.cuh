@@ -100,10 +100,21 @@ struct Sensor {
   float* raw;      // [nrec][ns] time series (nullptr: off)
   float* vmax;     // per-point reductions (nullptr: off)
   float* vmin;
-  float2* rms;     // Kahan sum of squares {sum, compensation}
+  float2* rms;     // sum of squares of the completed blocks, Kahan {sum, compensation}
+  float* rms_blk;  // plain sum of squares of the block in progress
   float* max_all;  // full-grid reductions (nullptr: off)
   float* min_all;
 };
+
+// The rms sum of squares is accumulated in blocks of kRmsBlock recorded
+// steps: within a block in a plain FP32 partial sum (4 bytes read and
+// written per point and step), and at each block's end the partial sum is
+// added to a Kahan-compensated total (8 more bytes each way, once per
+// block).  The rounding error stays near kRmsBlock ulp of the sum, where a
+// plain running sum over Nt steps reaches Nt ulp, and the per-step traffic
+// is half that of a Kahan pair updated every step.  Record index fi (1-based)
+// is the ((fi - 1) % kRmsBlock)-th step of its block.
+constexpr int kRmsBlock = 16;
 
 // Bounded waits of the row kernels (the mbarrier waits on their bulk
 // copies): time limit (0: the 2 s default) and the word a wait that runs

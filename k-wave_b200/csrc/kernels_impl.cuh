@@ -316,19 +316,39 @@ __device__ __forceinline__ long long raw_row(const Sensor& s, int fi) {
   return s.ring ? (long long)((fi - 1) % s.ring) : (long long)(fi - 1);
 }
 
+// Kahan-compensated addition of x to {sum, compensation}.
+__device__ __forceinline__ float2 kahan_acc(float2 acc, float x) {
+  const float y = x - acc.y;
+  const float t = acc.x + y;
+  acc.y = (t - acc.x) - y;
+  acc.x = t;
+  return acc;
+}
+
+// Position of record index fi in its rms block, and whether fi ends it.
+__device__ __forceinline__ int rms_pos(int fi) { return (fi - 1) % kRmsBlock; }
+
+// The block partial sum after adding v^2 (b: the partial sum so far, unread
+// at a block's first step).
+__device__ __forceinline__ float rms_step(int j, float b, float v) {
+  return j == 0 ? __fmul_rn(v, v) : __fmaf_rn(v, v, b);
+}
+
+// One recorded value into the blocked rms accumulators of `slot` (kRmsBlock).
+__device__ __forceinline__ void rms_put(const Sensor& s, int fi, long long slot, float v) {
+  const int j = rms_pos(fi);
+  const float b = rms_step(j, j ? s.rms_blk[slot] : 0.f, v);
+  if (j == kRmsBlock - 1)
+    s.rms[slot] = kahan_acc(fi == kRmsBlock ? make_float2(0.f, 0.f) : s.rms[slot], b);
+  else
+    s.rms_blk[slot] = b;
+}
+
 __device__ __forceinline__ void sensor_put(const Sensor& s, int fi, long long slot, float v) {
   if (s.raw) s.raw[raw_row(s, fi) * s.ns + slot] = v;
   if (s.vmax) s.vmax[slot] = (fi == 1) ? v : fmaxf(s.vmax[slot], v);
   if (s.vmin) s.vmin[slot] = (fi == 1) ? v : fminf(s.vmin[slot], v);
-  if (s.rms) {
-    // compensated (Kahan) running sum of squares
-    float2 acc = (fi == 1) ? make_float2(0.f, 0.f) : s.rms[slot];
-    const float y = v * v - acc.y;
-    const float t = acc.x + y;
-    acc.y = (t - acc.x) - y;
-    acc.x = t;
-    s.rms[slot] = acc;
-  }
+  if (s.rms) rms_put(s, fi, slot, v);
 }
 
 __device__ __forceinline__ void sensor_all(const Sensor& s, int fi, long long gi, float v) {
@@ -360,30 +380,38 @@ __device__ __forceinline__ float4 max4(float4 a, float4 b) {
 __device__ __forceinline__ float4 min4(float4 a, float4 b) {
   return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
 }
-__device__ __forceinline__ float2 kahan_add(float2 acc, float v) {
-  const float y = v * v - acc.y;
-  const float t = acc.x + y;
-  acc.y = (t - acc.x) - y;
-  acc.x = t;
-  return acc;
-}
-
 // Dense sensors and full-grid reductions for 4 consecutive points, split
 // into a load and a store part so that an epilogue issues every load of an
 // iteration (its own inputs and the accumulators) before any store: a store
 // through another pointer (p, say) would otherwise keep the accumulator loads
 // behind it, a second memory round trip per iteration.
-struct Acc4 {  // the accumulators loaded ahead: per-point max and the Kahan rms pair
-  float4 mx, r0, r1;
+struct Acc4 {  // the accumulators loaded ahead: per-point max and the rms block partial sums
+  float4 mx{}, bl{};
 };
+__device__ __forceinline__ void rms_load4(const Sensor& s, int fi, long long gi, Acc4& c) {
+  if (rms_pos(fi) != 0) c.bl = ld4(s.rms_blk, gi);
+}
+// (at a block's end the Kahan pairs are loaded here, once per kRmsBlock steps)
+__device__ __forceinline__ void rms_store4(const Sensor& s, int fi, long long gi, float4 v, const Acc4& c) {
+  const int j = rms_pos(fi);
+  const float4 b = make_float4(rms_step(j, c.bl.x, v.x), rms_step(j, c.bl.y, v.y), rms_step(j, c.bl.z, v.z),
+                               rms_step(j, c.bl.w, v.w));
+  if (j != kRmsBlock - 1) {
+    st4(s.rms_blk, gi, b);
+    return;
+  }
+  float4* r = reinterpret_cast<float4*>(s.rms + gi);
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 a = (fi == kRmsBlock) ? z : r[0], a2 = (fi == kRmsBlock) ? z : r[1];
+  const float2 t0 = kahan_acc(make_float2(a.x, a.y), b.x), t1 = kahan_acc(make_float2(a.z, a.w), b.y);
+  const float2 t2 = kahan_acc(make_float2(a2.x, a2.y), b.z), t3 = kahan_acc(make_float2(a2.z, a2.w), b.w);
+  r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
+  r[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+}
 __device__ __forceinline__ void sensor_dense4_load(const Sensor& s, int fi, long long gi, Acc4& c) {
   if (fi <= 1 || s.mode != 1) return;  // fi 1: the accumulators start here; <= 0: nothing recorded yet
   if (s.vmax) c.mx = ld4(s.vmax, gi);
-  if (s.rms) {
-    const float4* r = reinterpret_cast<const float4*>(s.rms + gi);
-    c.r0 = r[0];
-    c.r1 = r[1];
-  }
+  if (s.rms) rms_load4(s, fi, gi, c);
 }
 // (the less common accumulators -- per-point min, full-grid max / min -- are
 // loaded here, where they are updated)
@@ -393,15 +421,7 @@ __device__ __forceinline__ void sensor_dense4_store(const Sensor& s, int fi, lon
     if (s.raw) st4(s.raw, raw_row(s, fi) * s.ns + gi, v);
     if (s.vmax) st4(s.vmax, gi, fi == 1 ? v : max4(c.mx, v));
     if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
-    if (s.rms) {
-      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 a = (fi == 1) ? z : c.r0, b = (fi == 1) ? z : c.r1;
-      float2 t0 = kahan_add(make_float2(a.x, a.y), v.x), t1 = kahan_add(make_float2(a.z, a.w), v.y);
-      float2 t2 = kahan_add(make_float2(b.x, b.y), v.z), t3 = kahan_add(make_float2(b.z, b.w), v.w);
-      float4* r = reinterpret_cast<float4*>(s.rms + gi);
-      r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
-      r[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
-    }
+    if (s.rms) rms_store4(s, fi, gi, v, c);
   }
   if (s.max_all) st4(s.max_all, gi, fi == 1 ? v : max4(ld4(s.max_all, gi), v));
   if (s.min_all) st4(s.min_all, gi, fi == 1 ? v : min4(ld4(s.min_all, gi), v));
@@ -416,13 +436,9 @@ __device__ __forceinline__ void sensor_dense4(const Sensor& s, int fi, long long
     if (s.vmax) st4(s.vmax, gi, fi == 1 ? v : max4(ld4(s.vmax, gi), v));
     if (s.vmin) st4(s.vmin, gi, fi == 1 ? v : min4(ld4(s.vmin, gi), v));
     if (s.rms) {
-      float4* r = reinterpret_cast<float4*>(s.rms + gi);
-      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 a = (fi == 1) ? z : r[0], b = (fi == 1) ? z : r[1];
-      float2 t0 = kahan_add(make_float2(a.x, a.y), v.x), t1 = kahan_add(make_float2(a.z, a.w), v.y);
-      float2 t2 = kahan_add(make_float2(b.x, b.y), v.z), t3 = kahan_add(make_float2(b.z, b.w), v.w);
-      r[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
-      r[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+      Acc4 c;
+      rms_load4(s, fi, gi, c);
+      rms_store4(s, fi, gi, v, c);
     }
   }
   if (s.max_all) st4(s.max_all, gi, fi == 1 ? v : max4(ld4(s.max_all, gi), v));
@@ -493,7 +509,11 @@ struct TilePrefetch {
     if (s.mode != 1 || fi <= 1) return;
     field(s.vmax);
     field(s.vmin);
-    field(s.rms, 8);
+    if (s.rms) {
+      const int j = rms_pos(fi);
+      if (j != 0) field(s.rms_blk);
+      if (j == kRmsBlock - 1 && fi != kRmsBlock) field(s.rms, 8);
+    }
   }
 };
 
@@ -763,6 +783,28 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   }
 }
 
+// The split density rho_x + rho_y (+ rho_z) exists for the split-field PML:
+// where every PML factor of a point is 1 the split update summed over the
+// axes is rho - dt (2 rho + rho0 or rho0) sum_i du_i/dx_i, which needs only
+// the sum.  Such points store the sum in rho_x alone and leave rho_y, rho_z
+// untouched (16 bytes of traffic fewer per point and step in 3D).  The rule
+// is decided per aligned group of 4 x points (the vector epilogue's unit):
+// merged iff pml_y(y) == 1, pml_z(z) == 1 (3D) and pml_x == 1 on all of
+// x & ~3 .. (x & ~3) + 3 inside the row.  Every kernel that reads or writes
+// the density uses this rule.
+__device__ __forceinline__ bool row_in_pml(const float* const* pml, int dim, const Dims& d, long long row) {
+  return __ldg(pml[1] + (int)(row % d.ny)) != 1.f || (dim == 3 && __ldg(pml[2] + (int)(row / d.ny)) != 1.f);
+}
+
+__device__ __forceinline__ bool rho_merged(const float* const* pml, int dim, int nx, int x, int y, int z) {
+  if (__ldg(pml[1] + y) != 1.f) return false;
+  if (dim == 3 && __ldg(pml[2] + z) != 1.f) return false;
+  const int g = x & ~3, ge = min(g + 4, nx);
+  for (int j = g; j < ge; ++j)
+    if (__ldg(pml[0] + j) != 1.f) return false;
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // rho update and equation of state.  C2R of du_i/dx_i for every axis, split
 // mass conservation (linear / nonlinear), pressure sources, then either the
@@ -823,7 +865,12 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
         if (f + 1 < dim) {
           if (!bulk) pf.spectrum(a.S[f + 1]);
         } else {
-          _Pragma("unroll") for (int g = 0; g < dim; ++g) pf.field(a.rho[g]);
+          pf.field(a.rho[0]);
+          // rho_y, rho_z only where the tile has rows in the y or z PML (rows
+          // outside it read them at the x-PML ends only; a heuristic from
+          // the first and last row: it decides prefetching, not results)
+          if (row_in_pml(a.pml, dim, d, r0) || row_in_pml(a.pml, dim, d, r0 + tile_rows(d, r0, L) - 1))
+            _Pragma("unroll") for (int g = 1; g < dim; ++g) pf.field(a.rho[g]);
           pf.field(a.rho0.p);
           pf.field(a.c0sq.p);
           if (a.nonlinear) pf.field(a.bona.p);
@@ -887,7 +934,6 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       const long long gi = row * nx + x;
       const int y = (int)(row % d.ny), z = (int)(row / d.ny);
       float4 ro[3], pm4[3];
-      _Pragma("unroll") for (int f = 0; f < dim; ++f) ro[f] = ld4(a.rho[f], gi);
       pm4[0] = __ldg(reinterpret_cast<const float4*>(a.pml[0] + x));
       {
         const float vy = __ldg(a.pml[1] + y);
@@ -896,6 +942,14 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
           const float vz = __ldg(a.pml[2] + z);
           pm4[2] = make_float4(vz, vz, vz, vz);
         }
+      }
+      // outside the PML the density is stored merged (rho_merged)
+      const bool merged = pm4[0].x == 1.f && pm4[0].y == 1.f && pm4[0].z == 1.f && pm4[0].w == 1.f &&
+                          pm4[1].x == 1.f && (dim < 3 || pm4[2].x == 1.f);
+      if (merged) {
+        ro[0] = ld4(a.rho[0], gi);
+      } else {
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) ro[f] = ld4(a.rho[f], gi);
       }
       const float4 r0v4 = map4(a.rho0, gi);
       const float4 c24 = map4(a.c0sq, gi);
@@ -909,27 +963,36 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         auto c = [&](const float4& v) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); };
-        float du[3], rold[3];
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
-          du[f] = get_comp(D[f], lay, q, x + j);
-          rold[f] = c(ro[f]);
-        }
-        const float r0v = c(r0v4);
-        float rpr = r0v;
-        if (a.nonlinear) {
-          float rs = rold[0] + rold[1];
-          if (dim == 3) rs += rold[2];
-          rpr = 2.f * rs + r0v;
-        }
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
-          const float pm = c(pm4[f]);
-          rn[f][j] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
-          if (dense_on) rn[f][j] = rn[f][j] + damp * c(ds4);
-        }
-        float rsum = rn[0][j] + rn[1][j];
-        if (dim == 3) rsum += rn[2][j];
+        float du[3];
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) du[f] = get_comp(D[f], lay, q, x + j);
         float dsum = du[0] + du[1];
         if (dim == 3) dsum += du[2];
+        const float r0v = c(r0v4);
+        float rsum;
+        if (merged) {
+          // the split update summed over the axes, each PML factor 1
+          const float rold = c(ro[0]);
+          const float rpr = a.nonlinear ? 2.f * rold + r0v : r0v;
+          rsum = rold - a.dt * rpr * dsum;
+          if (dense_on) rsum = rsum + (float)dim * (damp * c(ds4));
+          rn[0][j] = rsum;
+        } else {
+          float rold[3];
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) rold[f] = c(ro[f]);
+          float rpr = r0v;
+          if (a.nonlinear) {
+            float rs = rold[0] + rold[1];
+            if (dim == 3) rs += rold[2];
+            rpr = 2.f * rs + r0v;
+          }
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+            const float pm = c(pm4[f]);
+            rn[f][j] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
+            if (dense_on) rn[f][j] = rn[f][j] + damp * c(ds4);
+          }
+          rsum = rn[0][j] + rn[1][j];
+          if (dim == 3) rsum += rn[2][j];
+        }
         float term = rsum;
         if (a.eos == 2) term = term + c(ta4) * r0v * dsum;
         if (a.nonlinear) term = term + c(bn4) * rsum * rsum / (2.f * r0v);
@@ -937,7 +1000,11 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
         outq[j] = r0v * dsum;
         outr[j] = rsum;
       }
-      _Pragma("unroll") for (int f = 0; f < dim; ++f) st4(a.rho[f], gi, make_float4(rn[f][0], rn[f][1], rn[f][2], rn[f][3]));
+      if (merged) {
+        st4(a.rho[0], gi, make_float4(rn[0][0], rn[0][1], rn[0][2], rn[0][3]));
+      } else {
+        _Pragma("unroll") for (int f = 0; f < dim; ++f) st4(a.rho[f], gi, make_float4(rn[f][0], rn[f][1], rn[f][2], rn[f][3]));
+      }
       const float4 pv4 = make_float4(outp[0], outp[1], outp[2], outp[3]);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -969,7 +1036,13 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
         const long long gi = __ldg(a.src.idx + j);
         const float v = src_value(a.src, a.src.sig, j, t);
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) a.rho[f][gi] = (a.src.mode == 0) ? v : a.rho[f][gi] + v;
+        const long long grow = gi / nx;
+        if (rho_merged(a.pml, dim, nx, (int)(gi - grow * nx), (int)(grow % d.ny), (int)(grow / d.ny))) {
+          const float vt = (float)dim * v;  // every component set to / increased by v
+          a.rho[0][gi] = (a.src.mode == 0) ? vt : a.rho[0][gi] + vt;
+        } else {
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) a.rho[f][gi] = (a.src.mode == 0) ? v : a.rho[f][gi] + v;
+        }
       }
       __syncthreads();
     }
@@ -984,33 +1057,48 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       const long long gi = row * nx + x;
       float du[3];
       _Pragma("unroll") for (int f = 0; f < dim; ++f) du[f] = get_comp(D[f], lay, q, x);
-      const float r0v = a.rho0.at(gi);
-      if (pass == 0) {
-        float rold[3];
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) rold[f] = a.rho[f][gi];
-        float rpr = r0v;
-        if (a.nonlinear) {
-          float rs = rold[0] + rold[1];
-          if (dim == 3) rs += rold[2];
-          rpr = 2.f * rs + r0v;
-        }
-        const int y = (int)(row % d.ny), z = (int)(row / d.ny);
-        const int coord[3] = {x, y, z};
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) {
-          const float pm = __ldg(a.pml[f] + coord[f]);
-          rnew[f] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
-          if (dense_on) rnew[f] = rnew[f] + damp * __ldg(a.dsrc.field + gi);
-          a.rho[f][gi] = rnew[f];
-        }
-        if (sp) continue;
-      } else {
-        _Pragma("unroll") for (int f = 0; f < dim; ++f) rnew[f] = a.rho[f][gi];
-      }
-      // equation of state (kspaceFirstOrder3D.m:963-1017)
-      float rsum = rnew[0] + rnew[1];
-      if (dim == 3) rsum += rnew[2];
       float dsum = du[0] + du[1];
       if (dim == 3) dsum += du[2];
+      const float r0v = a.rho0.at(gi);
+      const int y = (int)(row % d.ny), z = (int)(row / d.ny);
+      const bool merged = rho_merged(a.pml, dim, nx, x, y, z);
+      float rsum;
+      if (merged) {
+        if (pass == 0) {  // the split update summed over the axes, each PML factor 1
+          const float rold = a.rho[0][gi];
+          const float rpr = a.nonlinear ? 2.f * rold + r0v : r0v;
+          rsum = rold - a.dt * rpr * dsum;
+          if (dense_on) rsum = rsum + (float)dim * (damp * __ldg(a.dsrc.field + gi));
+          a.rho[0][gi] = rsum;
+          if (sp) continue;
+        } else {
+          rsum = a.rho[0][gi];
+        }
+      } else {
+        if (pass == 0) {
+          float rold[3];
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) rold[f] = a.rho[f][gi];
+          float rpr = r0v;
+          if (a.nonlinear) {
+            float rs = rold[0] + rold[1];
+            if (dim == 3) rs += rold[2];
+            rpr = 2.f * rs + r0v;
+          }
+          const int coord[3] = {x, y, z};
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) {
+            const float pm = __ldg(a.pml[f] + coord[f]);
+            rnew[f] = pm * (pm * rold[f] - a.dt * rpr * du[f]);
+            if (dense_on) rnew[f] = rnew[f] + damp * __ldg(a.dsrc.field + gi);
+            a.rho[f][gi] = rnew[f];
+          }
+          if (sp) continue;
+        } else {
+          _Pragma("unroll") for (int f = 0; f < dim; ++f) rnew[f] = a.rho[f][gi];
+        }
+        rsum = rnew[0] + rnew[1];
+        if (dim == 3) rsum += rnew[2];
+      }
+      // equation of state (kspaceFirstOrder3D.m:963-1017)
       const float c2 = a.c0sq.at(gi);
       float term = rsum;
       if (a.eos == 2) term = term + a.tau.at(gi) * r0v * dsum;

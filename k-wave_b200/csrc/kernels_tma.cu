@@ -76,6 +76,24 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
   __syncthreads();
   const int per_field = a.ncx * a.nouter;
   const int ntiles = a.nfields * per_field;
+  // Tiles are numbered f * per_field + r (field f, position r).  Without a
+  // derived field, block b takes tiles b, b + grid, ...  With one, block b
+  // takes positions b, b + grid, ... and at each position every field,
+  // the derived field first: its load from the source field and the source
+  // field's own load both come before the source tile is stored back in
+  // place, in one block's program order, and the second load hits L2.
+  const bool grouped = a.dual_field >= 0;
+  auto tile_at = [&](int k) -> int {  // this block's k-th tile, -1 past the end
+    if (!grouped) {
+      const int t = blockIdx.x + k * gridDim.x;
+      return t < ntiles ? t : -1;
+    }
+    const int q = k / a.nfields, j = k - q * a.nfields;
+    const int r = blockIdx.x + q * gridDim.x;
+    if (r >= per_field) return -1;
+    const int f = (j == 0) ? a.dual_field : (j - 1 < a.dual_field ? j - 1 : j);
+    return f * per_field + r;
+  };
   auto coords = [&](int t, int& f, int& x, int& y, int& z) {
     f = t / per_field;
     const int r = t - f * per_field;
@@ -93,7 +111,7 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
     coords(t, f, x, y, z);
     mbar_expect_tx(&bar[s], TTile<NC>::BYTES);
     if (t == a.wait.skip_tile) return;  // test hook: announced, never issued
-    tma_load_3d(bufs + s * E, &a.map[f], x, y, z, &bar[s]);
+    tma_load_3d(bufs + s * E, &a.map[f == a.dual_field ? a.dual_src : f], x, y, z, &bar[s]);
     inflight |= 1u << s;
     parity_bits = (parity_bits & ~(1u << s)) | ((unsigned)((j / ST) & 1) << s);
   };
@@ -102,13 +120,15 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
   pdl_wait();  // the fields are the predecessors' outputs
   pdl_trigger();
   if (threadIdx.x == 0) {
-    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
-    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+    const int t0 = tile_at(0), t1 = tile_at(1);
+    if (t0 >= 0) issue(t0, 0);
+    if (t1 >= 0) issue(t1, 1);
   }
   const ColLayout lay{TL};
   bool aborted = false;
-  int it = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+  for (int it = 0;; ++it) {
+    const int t = tile_at(it);
+    if (t < 0) break;
     const int s = it % ST;
     float2* b = bufs + s * E;
     const bool ok = mbar_wait(&bar[s], (it / ST) & 1, a.err, a.wait.limit_ns);
@@ -117,16 +137,23 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
       break;
     }
     if (threadIdx.x == 0) inflight &= ~(1u << s);
-    ct_fft<NC, INV, true, TL>(b, tw, lay);
+    int f, x, y, z;
+    coords(t, f, x, y, z);
+    if (f == a.dual_field) {  // the derived field: the first stage reads its input times the axis factor
+      const int l = threadIdx.x % TL, tid = threadIdx.x / TL;
+      const float2* tab = a.dual_tab;
+      ct_stage0_ld<NC, INV>(b, l, tid, lay, [&](int ll, int n) { return c_mul(b[lay(ll, n)], __ldg(tab + n)); });
+      ct_stages<NC, 1, INV>(b, tw, l, tid, lay);
+    } else {
+      ct_fft<NC, INV, true, TL>(b, tw, lay);
+    }
     fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      int f, x, y, z;
-      coords(t, f, x, y, z);
       tma_store_3d(&a.map[f], x, y, z, b);
       bulk_commit();
-      const int t2 = t + 2 * gridDim.x;
-      if (t2 < ntiles) {
+      const int t2 = tile_at(it + 2);
+      if (t2 >= 0) {
         bulk_wait_read<ST - 2>();  // the store out of the stage being refilled has read it
         issue(t2, it + 2);
       }

@@ -22,6 +22,13 @@ struct ColTmaArgs {
   int nouter;   // outer extent of this launch (z planes for the y pass)
   int outer0;   // first outer index
   int yaxis;    // 1: the transformed axis is the tensor's y dimension, 2: z
+  // Optional derived field (dual_field >= 0): its tiles are loaded from
+  // field dual_src, multiplied by dual_tab[position along the transformed
+  // axis] and transformed, then stored to its own map.  Tiles are then dealt
+  // field-fastest, so a source tile and its derived tile are loaded at about
+  // the same time and the second load is served by L2.
+  int dual_field, dual_src;
+  const float2* dual_tab;
   int* err;
   TmaWaitArgs wait;
 };

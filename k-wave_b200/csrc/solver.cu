@@ -49,7 +49,7 @@ cudaError_t launch_x_c2r(const float2* S, float* out, int accumulate, const Dims
 cudaError_t launch_scatter(float* f, const int* idx, const int* slot, int n, const float* sig,
                            int nrows_sig, int t, const float* weight, cudaStream_t st);
 cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim,
-                            long long n, cudaStream_t st);
+                            const float* const* pml, int nx, int ny, long long n, cudaStream_t st);
 cudaError_t launch_scale_rows(float* out, const float* in, const float* r, int nx, int ny, long long n,
                               cudaStream_t st);
 cudaError_t launch_interp_sensor(const Sensor& s, const float* vals, const int* vslot, const float* w, int K,
@@ -57,7 +57,8 @@ cudaError_t launch_interp_sensor(const Sensor& s, const float* vals, const int* 
 cudaError_t launch_record_field(const float* f, const Sensor& s, const Clock& clk, long long n,
                                 cudaStream_t st);
 cudaError_t launch_advance(int* t, cudaStream_t st);
-cudaError_t launch_rms_final(const float2* acc, float* out, long long n, float inv_n, cudaStream_t st);
+cudaError_t launch_rms_final(const float2* acc, const float* blk, int partial, float* out, long long n, float inv_n,
+                             cudaStream_t st);
 cudaError_t launch_medium_maps(float* c0_to_c0sq, float c0_scalar, float* ctau, float* ceta, const float* alpha,
                                float alpha_scalar, double np_per_db, double y, double tan_py, int eos, long long n,
                                cudaStream_t st);
@@ -861,13 +862,20 @@ void Session::corrected_source(float* out, const int* idx, const int* slot, int 
 
 // The y pass (3D) over z planes [z0, z0 + nzs) of the listed half-spectrum
 // buffers, forward or inverse.
-void Session::col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs) {
+// dual_field >= 0 (TMA-fed pass only): bufs[dual_field] is derived from
+// bufs[dual_src] times dual_tab along y as the pass runs (ColTmaArgs).
+void Session::col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs, int dual_field, int dual_src,
+                       const float2* dual_tab) {
   if (d.dim != 3 || bufs.empty()) return;
   const int n = (int)bufs.size();
+  if (dual_field >= 0 && !use_tma[1]) throw KwError(KW_ERR_INTERNAL, "derived field in a y pass without TMA");
   if (use_tma[1]) {
     ColTmaArgs ca;
     std::memset(&ca, 0, sizeof(ca));
     for (int i = 0; i < n; ++i) ca.map[i] = map_y[bufs[i]];
+    ca.dual_field = dual_field;
+    ca.dual_src = dual_src;
+    ca.dual_tab = dual_tab;
     ca.nfields = n;
     ca.ncx = (d.nxh + tma_lines(d.ny) - 1) / tma_lines(d.ny);
     ca.nouter = nzs;
@@ -966,11 +974,34 @@ void Session::run_spectral(std::vector<int> ins, std::vector<int> outs, std::vec
 // (the x factor is applied when the row kernel reads S1), S2 = ddy(ky) S1,
 // S3 = F_z^-1{ddz kappa F_z S0}.  In 2D the last axis is y: S1 as above,
 // S2 = F_y^-1{ddy kappa F_y S0}.
+// The y derivative of p (3D) is kappa P times the y derivative factor along
+// ky.  With the TMA-fed y pass that product is formed in the y-inverse pass
+// as kappa P's tiles are loaded (grad_col_inverse): the last-axis pass then
+// writes two fields instead of three and the y pass reads kappa P's tiles
+// twice, the second time from L2.  Otherwise the last-axis pass writes it as
+// a second output of kappa P.
+bool Session::grad_dual_in_y() const { return d.dim == 3 && use_tma[1]; }
+
 void Session::grad_pass() {
-  if (d.dim == 3)
-    fused_pass({0}, {1, 3}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 2}}, 2, {2, -1}, T.ddk_pos[1]);
-  else
+  if (d.dim == 3) {
+    if (grad_dual_in_y())
+      fused_pass({0}, {1, 3}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 2}}, 2);
+    else
+      fused_pass({0}, {1, 3}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 2}}, 2, {2, -1}, T.ddk_pos[1]);
+  } else {
     fused_pass({0}, {1, 2}, {SpecOp{OP_KAPPA, 0}, SpecOp{OP_GRAD_POS, 1}}, 2);
+  }
+}
+
+// The y-inverse pass of the gradient spectra S1..S3 over z planes [z0, z0 + nzs).
+void Session::grad_col_inverse(int z0, int nzs) {
+  if (grad_dual_in_y()) {
+    col_pass(true, {1, 3, 2}, z0, nzs, 2, 0, T.ddk_pos[1]);
+  } else {
+    std::vector<int> f;
+    for (int a = 0; a < d.dim; ++a) f.push_back(a + 1);
+    col_pass(true, f, z0, nzs);
+  }
 }
 
 // The y-inverse / row kernel / y-forward chain over z slabs; with two
@@ -1117,6 +1148,7 @@ void Session::setup_sensors(const kw_input* in) {
   if (opt.p_min) sens_p.vmin = (float*)zalloc(p_min_buf, per);
   if (opt.p_rms) {
     sens_p.rms = (float2*)zalloc(p_rms_buf, 2 * per);
+    sens_p.rms_blk = (float*)zalloc(p_rmsb_buf, per);
     zalloc(p_rmsf_buf, per);
   }
   if (opt.p_max_all) sens_p.max_all = (float*)zalloc(p_maxall_buf, all);
@@ -1128,6 +1160,7 @@ void Session::setup_sensors(const kw_input* in) {
     if (opt.u_min) sens_u[a].vmin = (float*)zalloc(u_min_buf[a], per);
     if (opt.u_rms) {
       sens_u[a].rms = (float2*)zalloc(u_rms_buf[a], 2 * per);
+      sens_u[a].rms_blk = (float*)zalloc(u_rmsb_buf[a], per);
       zalloc(u_rmsf_buf[a], per);
     }
     if (opt.u_max_all) sens_u[a].max_all = (float*)zalloc(u_maxall_buf[a], all);
@@ -1242,16 +1275,14 @@ void Session::enqueue_init() {
   interp_points(0);
   ++launches_;
   ck(launch_rho_init((float*)rho_buf[0].p, (float*)rho_buf[1].p, d.dim == 3 ? (float*)rho_buf[2].p : nullptr,
-                     p0d, c0sq_m, d.dim, d.npts, st), "rho init");
+                     p0d, c0sq_m, d.dim, pml_d, d.nx, d.ny, d.npts, st), "rho init");
   ++launches_;
   float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
   ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
   ++launches_;
   col_pass(false, {0}, 0, d.nz);
   grad_pass();
-  std::vector<int> outs;
-  for (int a = 0; a < d.dim; ++a) outs.push_back(a + 1);
-  col_pass(true, outs, 0, d.nz);
+  grad_col_inverse(0, d.nz);
   UArgs ua = u_args(S);
   ua.init = 1;
   ua.do_r2c = 0;
@@ -1353,7 +1384,7 @@ void Session::enqueue_step_body(uint64_t t) {
     }
     UArgs ua = u_args(S);
     for_slabs([&](int z0, int nzs) {
-      col_pass(true, f123, z0, nzs);
+      grad_col_inverse(z0, nzs);
       ck(launch_x_u(ua, slab_dims(z0, nzs), plan[0], twd[0], rowL, st), "x_u");
       ++launches_;
       col_pass(false, f123, z0, nzs);
@@ -1511,6 +1542,7 @@ std::vector<std::pair<std::string, DevBuf*>> Session::state_buffers() {
   v.push_back({"p_max", &p_max_buf});
   v.push_back({"p_min", &p_min_buf});
   v.push_back({"p_rms_acc", &p_rms_buf});
+  v.push_back({"p_rms_block", &p_rmsb_buf});
   v.push_back({"p_max_all", &p_maxall_buf});
   v.push_back({"p_min_all", &p_minall_buf});
   for (int a = 0; a < d.dim; ++a) {
@@ -1519,6 +1551,7 @@ std::vector<std::pair<std::string, DevBuf*>> Session::state_buffers() {
     v.push_back({u + "_max", &u_max_buf[a]});
     v.push_back({u + "_min", &u_min_buf[a]});
     v.push_back({u + "_rms_acc", &u_rms_buf[a]});
+    v.push_back({u + "_rms_block", &u_rmsb_buf[a]});
     v.push_back({u + "_max_all", &u_maxall_buf[a]});
     v.push_back({u + "_min_all", &u_minall_buf[a]});
     v.push_back({u + "_non_staggered", &uns_raw_buf[a]});
@@ -1645,9 +1678,16 @@ void Session::read(kw_output* out) {
   drain_raw(out);
   const long long nr = std::min<long long>(nrec, std::max<long long>(0, (long long)t_done - (long long)opt.start_index + 1));
   const float inv = nr > 0 ? 1.0f / (float)nr : 0.f;
-  if (p_rms_buf.p) ck(launch_rms_final((const float2*)p_rms_buf.p, (float*)p_rmsf_buf.p, ns, inv, st), "rms");
+  const int partial = (nr % kRmsBlock) != 0;  // a block of the blocked rms sum is still open
+  if (p_rms_buf.p)
+    ck(launch_rms_final((const float2*)p_rms_buf.p, (const float*)p_rmsb_buf.p, partial, (float*)p_rmsf_buf.p, ns,
+                        inv, st),
+       "rms");
   for (int a = 0; a < d.dim; ++a)
-    if (u_rms_buf[a].p) ck(launch_rms_final((const float2*)u_rms_buf[a].p, (float*)u_rmsf_buf[a].p, ns, inv, st), "rms");
+    if (u_rms_buf[a].p)
+      ck(launch_rms_final((const float2*)u_rms_buf[a].p, (const float*)u_rmsb_buf[a].p, partial,
+                          (float*)u_rmsf_buf[a].p, ns, inv, st),
+         "rms");
   const size_t ser = ring_rows ? 0 : (size_t)ns * (size_t)nrec, per = (size_t)ns;
   const size_t all = axisym ? (size_t)d.nx * ny0 : (size_t)d.npts;  // axisymmetric: the unmirrored quarter
   d2h(out->p, p_raw_buf.p, ser, st);

@@ -106,10 +106,13 @@ class Session {
   // them each step (kspaceFirstOrderAS.m:488-519, 709-722, 911-931)
   const kw_input* expand_axisymmetric(const kw_input* in);
   void run_spectral(std::vector<int> ins, std::vector<int> outs, std::vector<SpecOp> ops, int fanout);
-  void col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs);
+  void col_pass(bool inv, const std::vector<int>& bufs, int z0, int nzs, int dual_field = -1, int dual_src = -1,
+                const float2* dual_tab = nullptr);
   void fused_pass(const std::vector<int>& ins, const std::vector<int>& outs, const std::vector<SpecOp>& ops,
                   int fanout, const std::vector<int>& dual = {}, const float2* dual_tab = nullptr);
   void grad_pass();
+  bool grad_dual_in_y() const;
+  void grad_col_inverse(int z0, int nzs);
   Dims slab_dims(int z0, int nzs) const;
   void enqueue_init();
   void enqueue_step();
@@ -216,8 +219,9 @@ class Session {
   void interp_points(int which);  // 0: p, 1: u, 2: u on the regular grid
   DevBuf uns_raw_buf[3], uns_field_buf;  // its series; the shifted field of one component
   void record_non_staggered();
-  DevBuf p_raw_buf, p_max_buf, p_min_buf, p_rms_buf, p_rmsf_buf, p_maxall_buf, p_minall_buf;
-  DevBuf u_raw_buf[3], u_max_buf[3], u_min_buf[3], u_rms_buf[3], u_rmsf_buf[3], u_maxall_buf[3], u_minall_buf[3];
+  DevBuf p_raw_buf, p_max_buf, p_min_buf, p_rms_buf, p_rmsb_buf, p_rmsf_buf, p_maxall_buf, p_minall_buf;
+  DevBuf u_raw_buf[3], u_max_buf[3], u_min_buf[3], u_rms_buf[3], u_rmsb_buf[3], u_rmsf_buf[3], u_maxall_buf[3],
+      u_minall_buf[3];
 };
 
 // What tune_schedule() measured: the schedule chosen for the key, its device

@@ -47,7 +47,8 @@ def session_bytes(inp, record, sizes):
     b = int(sizes.device_bytes)
     rec = set(record)
     b += per_series * (("p" in rec) + dim * ("u" in rec) + dim * ("u_non_staggered" in rec))
-    b += 8 * ns * (("p_rms" in rec) + dim * ("u_rms" in rec)) + 4 * ns * 4
+    # rms: the Kahan pair of the completed blocks and the open block's partial sum
+    b += 12 * ns * (("p_rms" in rec) + dim * ("u_rms" in rec)) + 4 * ns * 4
     b += 4 * ng * sum(k in rec for k in ("p_max_all", "p_min_all", "p_final"))
     b += 4 * ng * dim * sum(k in rec for k in ("u_max_all", "u_min_all", "u_final"))
     return b
