@@ -783,28 +783,6 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   }
 }
 
-// The split density rho_x + rho_y (+ rho_z) exists for the split-field PML:
-// where every PML factor of a point is 1 the split update summed over the
-// axes is rho - dt (2 rho + rho0 or rho0) sum_i du_i/dx_i, which needs only
-// the sum.  Such points store the sum in rho_x alone and leave rho_y, rho_z
-// untouched (16 bytes of traffic fewer per point and step in 3D).  The rule
-// is decided per aligned group of 4 x points (the vector epilogue's unit):
-// merged iff pml_y(y) == 1, pml_z(z) == 1 (3D) and pml_x == 1 on all of
-// x & ~3 .. (x & ~3) + 3 inside the row.  Every kernel that reads or writes
-// the density uses this rule.
-__device__ __forceinline__ bool row_in_pml(const float* const* pml, int dim, const Dims& d, long long row) {
-  return __ldg(pml[1] + (int)(row % d.ny)) != 1.f || (dim == 3 && __ldg(pml[2] + (int)(row / d.ny)) != 1.f);
-}
-
-__device__ __forceinline__ bool rho_merged(const float* const* pml, int dim, int nx, int x, int y, int z) {
-  if (__ldg(pml[1] + y) != 1.f) return false;
-  if (dim == 3 && __ldg(pml[2] + z) != 1.f) return false;
-  const int g = x & ~3, ge = min(g + 4, nx);
-  for (int j = g; j < ge; ++j)
-    if (__ldg(pml[0] + j) != 1.f) return false;
-  return true;
-}
-
 // ---------------------------------------------------------------------------
 // rho update and equation of state.  C2R of du_i/dx_i for every axis, split
 // mass conservation (linear / nonlinear), pressure sources, then either the
@@ -869,7 +847,8 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
           // rho_y, rho_z only where the tile has rows in the y or z PML (rows
           // outside it read them at the x-PML ends only; a heuristic from
           // the first and last row: it decides prefetching, not results)
-          if (row_in_pml(a.pml, dim, d, r0) || row_in_pml(a.pml, dim, d, r0 + tile_rows(d, r0, L) - 1))
+          const long long rl = r0 + tile_rows(d, r0, L) - 1;
+          if (!a.box.row((int)(r0 % d.ny), (int)(r0 / d.ny), dim) || !a.box.row((int)(rl % d.ny), (int)(rl / d.ny), dim))
             _Pragma("unroll") for (int g = 1; g < dim; ++g) pf.field(a.rho[g]);
           pf.field(a.rho0.p);
           pf.field(a.c0sq.p);
@@ -943,9 +922,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
           pm4[2] = make_float4(vz, vz, vz, vz);
         }
       }
-      // outside the PML the density is stored merged (rho_merged)
-      const bool merged = pm4[0].x == 1.f && pm4[0].y == 1.f && pm4[0].z == 1.f && pm4[0].w == 1.f &&
-                          pm4[1].x == 1.f && (dim < 3 || pm4[2].x == 1.f);
+      const bool merged = a.box.at(x, y, z, dim);  // the density stored merged (RhoBox)
       if (merged) {
         ro[0] = ld4(a.rho[0], gi);
       } else {
@@ -1037,7 +1014,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
         const long long gi = __ldg(a.src.idx + j);
         const float v = src_value(a.src, a.src.sig, j, t);
         const long long grow = gi / nx;
-        if (rho_merged(a.pml, dim, nx, (int)(gi - grow * nx), (int)(grow % d.ny), (int)(grow / d.ny))) {
+        if (a.box.at((int)(gi - grow * nx), (int)(grow % d.ny), (int)(grow / d.ny), dim)) {
           const float vt = (float)dim * v;  // every component set to / increased by v
           a.rho[0][gi] = (a.src.mode == 0) ? vt : a.rho[0][gi] + vt;
         } else {
@@ -1061,7 +1038,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       if (dim == 3) dsum += du[2];
       const float r0v = a.rho0.at(gi);
       const int y = (int)(row % d.ny), z = (int)(row / d.ny);
-      const bool merged = rho_merged(a.pml, dim, nx, x, y, z);
+      const bool merged = a.box.at(x, y, z, dim);
       float rsum;
       if (merged) {
         if (pass == 0) {  // the split update summed over the axes, each PML factor 1

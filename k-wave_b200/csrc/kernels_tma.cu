@@ -312,13 +312,18 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
       }
       return ev;
     };
-    auto apply = [&](const OpEval& ev, float2 (&u)[M]) {
+    // prescaled: u already holds kappa * scale times the transform (GRAD)
+    auto apply = [&](const OpEval& ev, float2 (&u)[M], bool prescaled = false) {
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         const int p = tid + TPL * m;
         const float k2 = kxy2 + kl2[p];
         float f;
         if constexpr (CLS == FC_GRAD) {
+          if (prescaled) {
+            u[m] = c_mul(u[m], ev.dline ? ev.dline[p] : ev.dconst);
+            continue;
+          }
           f = ev.kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
           u[m] = c_mul(c_scale(u[m], f), ev.dline ? ev.dline[p] : ev.dconst);
         } else if constexpr (CLS == FC_NABLA) {
@@ -382,12 +387,25 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(
       // output is read from it in the hand-off order, multiplied in registers
       // and given the inverse first stage on the way to W
       ct_fft<NC, false, true, TL>(F, tw, lay);
+      // a first output of kappa alone (the gradient pass: kappa P, then kappa
+      // P times the axis derivative) leaves kappa * scale * F in F, so the
+      // later outputs carrying kappa skip its evaluation (c_mul by 1 + 0i is
+      // exact, so each output's value is unchanged)
+      bool kf = false;
 #pragma unroll 1
       for (int q = 0; q < a.fanout; ++q) {
         float2 u[M];
 #pragma unroll
         for (int m = 0; m < M; ++m) u[m] = F[lay(l, tid + TPL * m)];
-        apply(setup(q), u);
+        const OpEval ev = setup(q);
+        apply(ev, u, kf && ev.kappa);
+        if constexpr (CLS == FC_GRAD) {
+          if (q == 0 && a.fanout > 1 && a.op[g * a.fanout].kind == OP_KAPPA) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) F[lay(l, tid + TPL * m)] = u[m];  // this thread's own positions
+            kf = true;
+          }
+        }
         ct_inv_first_from_regs<NC>(u, W, l, tid, lay);
         if (q + 1 == a.fanout) fence_async_smem();
         __syncthreads();

@@ -48,8 +48,8 @@ cudaError_t launch_x_c2r(const float2* S, float* out, int accumulate, const Dims
                          const float2* tw, int L, cudaStream_t st);
 cudaError_t launch_scatter(float* f, const int* idx, const int* slot, int n, const float* sig,
                            int nrows_sig, int t, const float* weight, cudaStream_t st);
-cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim,
-                            const float* const* pml, int nx, int ny, long long n, cudaStream_t st);
+cudaError_t launch_rho_init(float* r0, float* r1, float* r2, const float* p0, Map c0sq, int dim, const RhoBox& box,
+                            int nx, int ny, long long n, cudaStream_t st);
 cudaError_t launch_scale_rows(float* out, const float* in, const float* r, int nx, int ny, long long n,
                               cudaStream_t st);
 cudaError_t launch_interp_sensor(const Sensor& s, const float* vals, const int* vslot, const float* w, int K,
@@ -514,6 +514,18 @@ void Session::setup(const kw_input* in, const kw_options* o, bool allow_ring) {
       pms = pml_profile(ns[a], dd[a], dt, c_ref, (int)psz[a], pal[a], true);
     }
     std::vector<float> f1(pm.begin(), pm.end()), f2(pms.begin(), pms.end());
+    {  // the merged-density box along this axis: the first run of PML factors equal to 1
+      int lo = 0;
+      while (lo < (int)f1.size() && f1[lo] != 1.f) ++lo;
+      int hi = lo;
+      while (hi < (int)f1.size() && f1[hi] == 1.f) ++hi;
+      if (a == 0) {  // whole aligned groups of 4 x points
+        lo = (lo + 3) & ~3;
+        hi &= ~3;
+      }
+      rho_box.lo[a] = lo;
+      rho_box.hi[a] = std::max(lo, hi);
+    }
     pml_d[a] = up(pml_buf[a], f1.data(), f1.size(), st);
     pml_sg_d[a] = up(pmls_buf[a], f2.data(), f2.size(), st);
   }
@@ -1275,7 +1287,7 @@ void Session::enqueue_init() {
   interp_points(0);
   ++launches_;
   ck(launch_rho_init((float*)rho_buf[0].p, (float*)rho_buf[1].p, d.dim == 3 ? (float*)rho_buf[2].p : nullptr,
-                     p0d, c0sq_m, d.dim, pml_d, d.nx, d.ny, d.npts, st), "rho init");
+                     p0d, c0sq_m, d.dim, rho_box, d.nx, d.ny, d.npts, st), "rho init");
   ++launches_;
   float2* S[4] = {(float2*)S_buf[0].p, (float2*)S_buf[1].p, (float2*)S_buf[2].p, (float2*)S_buf[3].p};
   ck(launch_x_r2c(p0d, S[0], d, plan[0], twd[0], rowL, st), "x_r2c");
@@ -1422,6 +1434,7 @@ void Session::enqueue_step_body(uint64_t t) {
       ra.pml[a] = pml_d[a];
     }
     ra.rho0 = rho0_m;
+    ra.box = rho_box;
     ra.dt = dtf;
     ra.nonlinear = nonlinear;
     ra.bona = bona_m;

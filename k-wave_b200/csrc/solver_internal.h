@@ -157,6 +157,7 @@ class Session {
   // operator tables
   DevBuf tw_buf[3], k2_buf[3], pos_buf[3], neg_buf[3], sh_buf[3], pml_buf[3], pmls_buf[3];
   const float* pml_d[3]{};
+  RhoBox rho_box{};  // merged-density points (RhoBox)
   const float* pml_sg_d[3]{};
   // medium
   DevBuf c0sq_buf, rho0_buf, rinv_buf[3], bona_buf, c2tau_buf, c2eta_buf;
