@@ -59,6 +59,32 @@ def ct_sizes():
         return [int(v) for v in re.findall(r"X\((\d+)\)", f.read())]
 
 
+def tma_sizes():
+    """Transform lengths listed in csrc/tma_sizes.h."""
+    import re
+
+    with open(os.path.join(CSRC, "tma_sizes.h")) as f:
+        return [int(v) for v in re.findall(r"X\((\d+)\)", f.read())]
+
+
+def _fused_sources():
+    """One generated translation unit per TMA length: an explicit
+    instantiation of the fused last-axis pass fused_tma_cls<N> (fused_tma.cuh)."""
+    d = os.path.join(BUILD, "tma")
+    os.makedirs(d, exist_ok=True)
+    out = []
+    for n in tma_sizes():
+        path = os.path.join(d, f"fused_tma_{n}.cu")
+        text = (f'#include "fused_tma.cuh"\nnamespace kwb {{\n'
+                f'template cudaError_t fused_tma_cls<{n}>(const FusedTmaArgs&, const float2*, const SpecTables&,'
+                f' cudaStream_t);\n}}\n')
+        if not os.path.exists(path) or open(path).read() != text:
+            with open(path, "w") as f:
+                f.write(text)
+        out.append(path)
+    return out
+
+
 def _ct_sources():
     """One generated translation unit per compile-time length: an explicit
     instantiation of CtKernels<N> (kernels_impl.cuh)."""
@@ -81,7 +107,7 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
     hdrs = _headers()
     jobs_list = []
     objs = []
-    for s in _ct_sources():
+    for s in _ct_sources() + _fused_sources():
         o = s[:-3] + ".o"
         objs.append(o)
         if force or _stale(o, [s] + hdrs):

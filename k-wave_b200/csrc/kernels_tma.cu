@@ -1,7 +1,7 @@
-// Persistent, TMA-fed column passes (the y pass and the fused last-axis
-// operator) for compile-time transform lengths up to 256 (the y pass: every
-// 2^a 3^b 5^c length from 64 to 256; the fused operator: the two-stage
-// lengths 64, 128, 256, whose register hand-off it is built on).
+// Persistent, TMA-fed column passes for the compile-time transform lengths
+// of tma_sizes.h (every 2^a 3^b 5^c length from 64 to 256): the y pass
+// here, the fused last-axis operator in fused_tma.cuh (instantiated per
+// length in generated translation units), and the host side of both.
 //
 // Each thread block loops over column tiles (TL adjacent kx columns x the
 // whole line).  Tiles arrive by cp.async.bulk.tensor into a ring of shared
@@ -15,42 +15,14 @@
 #include <algorithm>
 
 #include "fft_ct.cuh"
+#include "fused_tma.cuh"
 #include "kernels.cuh"
 #include "kernels_tma.cuh"
 #include "spec_ops.cuh"
 #include "tma.cuh"
+#include "tma_sizes.h"
 
 namespace kwb {
-
-// Lines per TMA tile: the compile-time tile's line count rounded down to an
-// even number, so every tile starts at a bin index x = cx * LINES whose byte
-// offset (8-byte bins) is a multiple of 16, as tensor copies require.
-__host__ __device__ constexpr int tma_lines_of(int n) {
-  return ct_lines_of(n) & ~1;  // ct_lines_of is at least 4
-}
-
-template <int NC>
-struct TTile {
-  static constexpr int LINES = tma_lines_of(NC);
-  static constexpr int THREADS = Ct<NC>::T * LINES;
-  static constexpr int ELEMS = LINES * NC;
-  static constexpr unsigned BYTES = ELEMS * sizeof(float2);
-  // Stage stride in elements: tensor copies read and write shared memory at
-  // 128-byte aligned addresses, so each stage is padded to a multiple of 128
-  // bytes (a tile of 14 lines of 90 points is 10080 bytes).
-  static constexpr int STRIDE = (int)((BYTES + 127u) / 128u * 128u / sizeof(float2));
-};
-
-__device__ __forceinline__ void tile_coords(int yaxis, int cx, int o, int lines, int& x, int& y, int& z) {
-  x = cx * lines;
-  if (yaxis == 1) {
-    y = 0;
-    z = o;
-  } else {
-    y = o;
-    z = 0;
-  }
-}
 
 // Shared-memory stages of the y pass: tiles t + grid and t + 2 grid load
 // while tile t is transformed and stored (two blocks per SM at 256 points).
@@ -167,258 +139,6 @@ __global__ void __launch_bounds__(TTile<NC>::THREADS) k_col_tma(const __grid_con
   }
 }
 
-// Operator classes of the fused kernel: one instantiation per class keeps
-// only that operator's arithmetic in the kernel body.
-enum FusedClass { FC_GRAD = 0, FC_NABLA = 1, FC_SRCK = 2 };
-
-// MODE 1: every input has a single output (the register hand-off path, in
-// place in the input stage: two tile buffers, three blocks per SM).
-// MODE 0: the forward transform is kept and each output multiplied from it
-// into a third buffer (two blocks per SM).  (The gradient's pair of outputs,
-// kappa and kappa times the transform axis' derivative, also fits the
-// in-place form with both taken from the hand-off registers, but at three
-// blocks per SM that spills and measured slower: 1.338 against 1.330 ms.)
-template <int NC, int CLS, int MODE>
-__global__ void __launch_bounds__(TTile<NC>::THREADS, MODE ? 3 : 2) k_fused_tma(const __grid_constant__ FusedTmaArgs a,
-                                                                     const float2* __restrict__ tw_g,
-                                                                     const __grid_constant__ SpecTables T) {
-  constexpr int TL = TTile<NC>::LINES;
-  constexpr int E = TTile<NC>::ELEMS;
-  constexpr int TH = TTile<NC>::THREADS;
-  static_assert(Ct<NC>::S == 2, "the fused last-axis kernel assumes a two-stage plan");
-  static_assert(TTile<NC>::STRIDE == E, "tile buffers must start at 128-byte aligned addresses");
-  extern __shared__ __align__(128) unsigned char smraw[];
-  float2* inb = reinterpret_cast<float2*>(smraw);  // 2 input stages
-  float2* W = MODE ? nullptr : inb + 2 * E;        // product / inverse-transform buffer (MODE 0)
-  float2* tw = inb + (MODE ? 2 : 3) * E;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + NC);
-  // per-line tables of the transform axis: shifted derivatives (+, -) and k^2
-  float2* dpos = reinterpret_cast<float2*>(bar + 2);
-  float2* dneg = dpos + NC;
-  float2* dsh = dneg + NC;
-  float* kl2 = reinterpret_cast<float*>(dsh + NC);
-  if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    fence_mbar_init();
-  }
-  const int lax = (a.dim == 3) ? 2 : 1;
-  for (int i = threadIdx.x; i < NC; i += blockDim.x) {
-    tw[i] = tw_g[i];
-    kl2[i] = T.k2[lax][i];
-    if constexpr (CLS == FC_GRAD) {
-      dpos[i] = T.ddk_pos[lax][i];
-      dneg[i] = T.ddk_neg[lax][i];
-      dsh[i] = T.shift_neg[lax] ? T.shift_neg[lax][i] : make_float2(1.f, 0.f);
-    }
-  }
-  __syncthreads();
-  const int main_in = a.ncx * a.nouter;  // column tiles of one input
-  const int per_in = main_in + a.nrem;
-  const int ntiles = a.nin * per_in;
-  // tile t -> input g and, for a column tile, its first column cx and outer
-  // index o; a remainder tile has cx = -1 and its first outer index in o
-  auto decode = [&](int t, int& g, int& cx, int& o) {
-    g = t / per_in;
-    const int r = t - g * per_in;
-    if (r < main_in) {
-      o = r / a.ncx;
-      cx = r - o * a.ncx;
-    } else {
-      cx = -1;
-      o = (r - main_in) * a.rem_y;
-    }
-  };
-  __shared__ unsigned inflight, parity_bits;  // thread 0: as in k_col_tma
-  if (threadIdx.x == 0) inflight = parity_bits = 0;
-  auto issue = [&](int t, int j) {  // tile t, consumed at loop iteration j
-    const int s = j & 1;
-    int g, cx, o, x, y, z;
-    decode(t, g, cx, o);
-    mbar_expect_tx(&bar[s], TTile<NC>::BYTES);  // a remainder box holds as many bytes
-    if (t == a.wait.skip_tile) return;  // test hook: announced, never issued
-    if (cx >= 0) {
-      tile_coords(a.yaxis, cx, o, TL, x, y, z);
-      tma_load_3d(inb + s * E, &a.in[g], x, y, z, &bar[s]);
-    } else {
-      tma_load_3d(inb + s * E, &a.in_rem[g], a.ncols - 1, o, 0, &bar[s]);
-    }
-    inflight |= 1u << s;
-    parity_bits = (parity_bits & ~(1u << s)) | ((unsigned)((j >> 1) & 1) << s);
-  };
-  pdl_wait();  // the inputs are the predecessors' outputs
-  pdl_trigger();
-  if (threadIdx.x == 0) {
-    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
-    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
-  }
-  const ColLayout lay{TL};
-  // the line mapping fixes this thread's column (kx) for every pass
-  const int l = threadIdx.x % TL, tid = threadIdx.x / TL;
-  const float cdt2sq = T.cdt2 * T.cdt2;
-  constexpr int TPL = TH / TL;  // threads per line
-  constexpr int M = CtHandoff<NC>::M;
-  static_assert(TPL == Ct<NC>::T, "one line per group of T threads");
-  bool aborted = false;
-  int it = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-    const int s = it & 1;
-    float2* F = inb + s * E;
-    int g, cx, o;
-    decode(t, g, cx, o);
-    // this thread's line: its column ix and outer index ol, where its
-    // output goes (loff) and whether it is a real column (valid)
-    int ix, ol;
-    long long loff;
-    bool valid;
-    if (cx >= 0) {
-      const int x0 = cx * TL;
-      ix = min(x0 + l, a.ncols - 1);
-      ol = o;
-      loff = (long long)o * a.ostride + x0 + l;
-      valid = (x0 + l) < a.ncols;
-    } else {  // lines alternate the last column and the padding bin
-      ix = a.ncols - 1;
-      ol = o + (l >> 1);
-      loff = (long long)ol * a.ostride + ix;
-      valid = (l & 1) == 0;
-    }
-    const float kxy2 = __ldg(T.k2[0] + ix) + ((a.dim == 3) ? __ldg(T.k2[1] + ol) : 0.f);
-    // the operator of output q: a real factor m(|k|^2), times a complex
-    // factor that is constant along the line or read from a line table
-    struct OpEval {
-      float2 dconst;
-      const float2* dline;
-      float e;
-      bool kappa;
-    };
-    auto setup = [&](int q) {
-      const SpecOp op = a.op[g * a.fanout + q];
-      OpEval ev{make_float2(1.f, 0.f), nullptr, 0.f, true};
-      if constexpr (CLS == FC_GRAD) {
-        if (op.kind != OP_KAPPA) {
-          ev.kappa = op.kind != OP_SHIFT_NEG;  // the shift operator carries no kappa
-          if (op.axis == lax) {
-            ev.dline = (op.kind == OP_GRAD_POS) ? dpos : (op.kind == OP_GRAD_NEG ? dneg : dsh);
-          } else {
-            const float2* tab = (op.kind == OP_GRAD_POS)   ? T.ddk_pos[op.axis]
-                                : (op.kind == OP_GRAD_NEG) ? T.ddk_neg[op.axis]
-                                                           : T.shift_neg[op.axis];  // shift, kappa * shift
-            ev.dconst = __ldg(tab + (op.axis == 0 ? ix : ol));
-          }
-        }
-      } else if constexpr (CLS == FC_NABLA) {
-        ev.e = 0.5f * ((op.kind == OP_NABLA1) ? T.ym2 : T.ym1);  // |k|^y = (|k|^2)^(y/2)
-      }
-      return ev;
-    };
-    // prescaled: u already holds kappa * scale times the transform (GRAD)
-    auto apply = [&](const OpEval& ev, float2 (&u)[M], bool prescaled = false) {
-#pragma unroll
-      for (int m = 0; m < M; ++m) {
-        const int p = tid + TPL * m;
-        const float k2 = kxy2 + kl2[p];
-        float f;
-        if constexpr (CLS == FC_GRAD) {
-          if (prescaled) {
-            u[m] = c_mul(u[m], ev.dline ? ev.dline[p] : ev.dconst);
-            continue;
-          }
-          f = ev.kappa ? sinc_sq(cdt2sq * k2) * T.scale : T.scale;
-          u[m] = c_mul(c_scale(u[m], f), ev.dline ? ev.dline[p] : ev.dconst);
-        } else if constexpr (CLS == FC_NABLA) {
-          f = (k2 == 0.f) ? (ev.e == 0.f ? T.scale : 0.f) : exp2f(ev.e * log2f(k2)) * T.scale;
-          u[m] = c_scale(u[m], f);
-        } else {
-          f = cos_sq(cdt2sq * k2) * T.scale;
-          u[m] = c_scale(u[m], f);
-        }
-      }
-    };
-    // inverse last stage, straight from W to the output (and the optional
-    // second output scaled by a factor constant along the line)
-    auto finish = [&](int q, const float2* src) {
-      float2* dst = a.outp[g * a.fanout + q] + loff;
-      float2* dst2 = a.dual_outp[g * a.fanout + q];
-      float2 dsc = make_float2(0.f, 0.f);
-      if (dst2) {
-        dst2 += loff;
-        dsc = __ldg(a.dual_tab[g * a.fanout + q] + ol);
-      }
-      auto ld_w = [&](int ll, int pos) -> float2 { return src[lay(ll, pos)]; };
-      auto st_g = [&](int, int pos, float2 v) {  // (the line is this thread's, folded into loff)
-        if (valid) {
-          dst[pos * a.lstride] = v;
-          if (dst2) dst2[pos * a.lstride] = c_mul(v, dsc);
-        }
-      };
-      ct_stage_io<NC, 1, true>(tw, l, tid, ld_w, st_g);
-      fence_async_smem();  // the reads of src come before a TMA refill of it
-      __syncthreads();     // src is reused by the next inverse
-    };
-    auto refill = [&]() {  // F is consumed: refill this input stage with the tile two ahead
-      if (threadIdx.x == 0) {
-        const int t2 = t + 2 * gridDim.x;
-        if (t2 < ntiles) issue(t2, it + 2);
-      }
-    };
-    const bool ok = mbar_wait(&bar[s], (it >> 1) & 1, a.err, a.wait.limit_ns);
-    if (__syncthreads_or(!ok)) {  // every thread leaves together; nothing more is issued
-      aborted = true;
-      break;
-    }
-    if (threadIdx.x == 0) inflight &= ~(1u << s);
-    if constexpr (MODE == 1) {
-      float2 u[M];
-      // forward first stage in place; last stage, operator and inverse first
-      // stage in registers, the latter's outputs back into F once every
-      // thread has read its inputs; inverse last stage to the output; then F
-      // takes the tile two ahead
-      ct_stage<NC, 0, false>(F, tw, l, tid, lay);
-      ct_fwd_last_to_regs<NC>(F, tw, l, tid, lay, u);
-      apply(setup(0), u);
-      __syncthreads();
-      ct_inv_first_from_regs<NC>(u, F, l, tid, lay);
-      __syncthreads();
-      finish(0, F);
-      refill();
-    } else {
-      // several outputs of one input: the forward transform stays in F; each
-      // output is read from it in the hand-off order, multiplied in registers
-      // and given the inverse first stage on the way to W
-      ct_fft<NC, false, true, TL>(F, tw, lay);
-      // a first output of kappa alone (the gradient pass: kappa P, then kappa
-      // P times the axis derivative) leaves kappa * scale * F in F, so the
-      // later outputs carrying kappa skip its evaluation (c_mul by 1 + 0i is
-      // exact, so each output's value is unchanged)
-      bool kf = false;
-#pragma unroll 1
-      for (int q = 0; q < a.fanout; ++q) {
-        float2 u[M];
-#pragma unroll
-        for (int m = 0; m < M; ++m) u[m] = F[lay(l, tid + TPL * m)];
-        const OpEval ev = setup(q);
-        apply(ev, u, kf && ev.kappa);
-        if constexpr (CLS == FC_GRAD) {
-          if (q == 0 && a.fanout > 1 && a.op[g * a.fanout].kind == OP_KAPPA) {
-#pragma unroll
-            for (int m = 0; m < M; ++m) F[lay(l, tid + TPL * m)] = u[m];  // this thread's own positions
-            kf = true;
-          }
-        }
-        ct_inv_first_from_regs<NC>(u, W, l, tid, lay);
-        if (q + 1 == a.fanout) fence_async_smem();
-        __syncthreads();
-        if (q + 1 == a.fanout) refill();
-        finish(q, W);
-      }
-    }
-  }
-  if (threadIdx.x == 0 && aborted)  // the loads still in flight land before shared memory is released
-    for (int s = 0; s < 2; ++s)
-      if (inflight & (1u << s)) mbar_wait(&bar[s], (parity_bits >> s) & 1, nullptr, a.wait.limit_ns);
-}
-
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -434,11 +154,6 @@ static bool get_encoder() {
   return true;
 }
 
-// TMA-fed y pass lengths (the box's line extent is at most 256 elements)
-#define KWB_TMA_COL_SIZES(X)                                                                                   \
-  X(64) X(72) X(75) X(80) X(81) X(90) X(96) X(100) X(108) X(120) X(125) X(128) X(135) X(144) X(150) X(160) \
-  X(162) X(180) X(192) X(200) X(216) X(225) X(240) X(243) X(250) X(256)
-
 bool tma_col_supported(int n) {
   switch (n) {
 #define KWB_CASE(N) case N:
@@ -450,7 +165,7 @@ bool tma_col_supported(int n) {
   }
 }
 
-bool tma_fused_supported(int n) { return n == 64 || n == 128 || n == 256; }
+bool tma_fused_supported(int n) { return tma_col_supported(n); }
 
 // Tensor map over a half-spectrum buffer [nz][ny][nxp] (8-byte elements),
 // box {lines, ny or 1, 1 or nz} for transforms along y (yaxis 1) or z (2).
@@ -489,7 +204,7 @@ bool make_spec_map_rem(CUtensorMap* m, void* base, const Dims& d, int n, int row
 }
 
 static int g_num_sms = 0;
-static int num_sms() {
+int tma_num_sms() {
   if (!g_num_sms) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -506,36 +221,9 @@ static cudaError_t col_tma_t(const ColTmaArgs& a, const float2* tw, cudaStream_t
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
   const int ntiles = a.nfields * a.ncx * a.nouter;
-  const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
+  const int grid = std::min(ntiles, std::max(1, per_sm) * tma_num_sms());
   const cudaError_t e = launch_pdl(k, dim3(grid), dim3(TTile<NC>::THREADS), sm, st, a, tw);
   return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-template <int NC, int CLS, int MODE>
-static cudaError_t fused_tma_t(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
-  const size_t sm = (MODE ? 2 : 3) * TTile<NC>::BYTES + NC * sizeof(float2) + 2 * sizeof(uint64_t) + 3 * NC * sizeof(float2) +
-                    NC * sizeof(float);
-  auto k = k_fused_tma<NC, CLS, MODE>;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TTile<NC>::THREADS, sm);
-  const int ntiles = a.nin * (a.ncx * a.nouter + a.nrem);
-  const int grid = std::min(ntiles, std::max(1, per_sm) * num_sms());
-  const cudaError_t e = launch_pdl(k, dim3(grid), dim3(TTile<NC>::THREADS), sm, st, a, tw, T);
-  return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-template <int NC>
-static cudaError_t fused_tma_cls(const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
-  const int kind = a.op[0].kind;
-  const bool one = a.fanout == 1;
-  if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG || kind == OP_KAPPA || kind == OP_SHIFT_NEG ||
-      kind == OP_KAPPA_SHIFT_NEG) {
-    return one ? fused_tma_t<NC, FC_GRAD, 1>(a, tw, T, st) : fused_tma_t<NC, FC_GRAD, 0>(a, tw, T, st);
-  }
-  if (kind == OP_NABLA1 || kind == OP_NABLA2)
-    return one ? fused_tma_t<NC, FC_NABLA, 1>(a, tw, T, st) : fused_tma_t<NC, FC_NABLA, 0>(a, tw, T, st);
-  return one ? fused_tma_t<NC, FC_SRCK, 1>(a, tw, T, st) : fused_tma_t<NC, FC_SRCK, 0>(a, tw, T, st);
 }
 
 int tma_lines(int n) { return tma_lines_of(n); }
@@ -554,10 +242,13 @@ cudaError_t launch_col_tma(bool inv, int n, const ColTmaArgs& a, const float2* t
 
 cudaError_t launch_fused_tma(int n, const FusedTmaArgs& a, const float2* tw, const SpecTables& T, cudaStream_t st) {
   switch (n) {
-    case 64: return fused_tma_cls<64>(a, tw, T, st);
-    case 128: return fused_tma_cls<128>(a, tw, T, st);
-    case 256: return fused_tma_cls<256>(a, tw, T, st);
-    default: return cudaErrorInvalidValue;
+#define KWB_CASE(N) \
+  case N:           \
+    return fused_tma_cls<N>(a, tw, T, st);
+    KWB_TMA_COL_SIZES(KWB_CASE)
+#undef KWB_CASE
+    default:
+      return cudaErrorInvalidValue;
   }
 }
 

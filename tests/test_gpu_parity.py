@@ -192,6 +192,15 @@ def test_3d_compile_time_mixed_radix_sizes(n):
     _check(inp, record, TOL)
 
 
+@pytest.mark.parametrize("nz", [80, 81, 96, 125, 144, 162, 192, 243, 250])
+def test_tma_last_axis_operator_on_multi_stage_lengths(nz):
+    """The TMA-fed last-axis operator on 2^a 3^b 5^c lengths other than 64,
+    128 and 256 (forward transform, operator and inverse through shared
+    memory, no register hand-off), against the oracle."""
+    inp, record, start, _ = case_3d_het(n=(32, 30, nz), nt=12, record=("p", "p_max", "p_rms", "u", "p_final"))
+    _check(inp, record, TOL)
+
+
 @pytest.mark.parametrize("n", [(56, 42), (112, 49), (98, 70)])
 def test_2d_radix7_sizes(n):
     """Edges with a factor 7 (the runtime FFT engine's radix-7 stage)."""
