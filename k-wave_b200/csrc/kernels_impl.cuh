@@ -607,7 +607,10 @@ struct RawRows {
 // u update: C2R of the gradient, split-PML momentum update, velocity
 // sources, velocity sensors, R2C of the new velocity.  blockIdx.y = axis.
 // ---------------------------------------------------------------------------
-template <int NC>
+// LEAN: the variant for steps with no velocity source and no velocity sensor
+// after the first (no source, sensor or initial-pressure code: a smaller
+// kernel body); otherwise every case.
+template <int NC, bool LEAN>
 __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
                                                            const __grid_constant__ FFTPlan plan,
                                                            const float2* __restrict__ tw_g, int Lrt) {
@@ -637,12 +640,13 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
     if (threadIdx.x < 32) bulk_rows(B0, a.S[ax], d, r0, tile_rows(d, r0, L), &rbar[0]);
   }
   const int t = *a.clk.t;
-  const int fi = record_index(a.clk);
+  const int fi = LEAN ? 0 : record_index(a.clk);
+  const bool init = !LEAN && a.init;
   float2* G;
   if constexpr (RowBulk<NC>::OK) {
     {  // the epilogue's inputs stream in during the wait and the FFT
       TilePrefetch pf(d, r0, L);
-      if (!a.init) pf.field(a.u[ax]);
+      if (!init) pf.field(a.u[ax]);
       pf.field(a.rinv[ax].p);
       pf.sensor(a.sens[ax], fi);
     }
@@ -657,7 +661,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
     __syncthreads();
     if constexpr (NC > 0 && NC % 4 == 0) {  // the epilogue's inputs stream in during the FFT
       TilePrefetch pf(d, r0, L);
-      if (!a.init) pf.field(a.u[ax]);
+      if (!init) pf.field(a.u[ax]);
       pf.field(a.rinv[ax].p);
       pf.sensor(a.sens[ax], fi);
     }
@@ -668,7 +672,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   const float* pml = a.pml_sg[ax];
   const Map rinv = a.rinv[ax];
   const DenseSource ds = a.dsrc[ax];
-  const bool dense_on = ds.field && t <= ds.len;
+  const bool dense_on = !LEAN && ds.field && t <= ds.len;
   const float damp = dense_on ? (ds.sig ? __ldg(ds.sig + t - 1) : 1.f) : 0.f;
   const int total = 2 * L * nx;
   constexpr bool VEC = NC > 0 && NC % 4 == 0;
@@ -692,7 +696,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
         pm = make_float4(v, v, v, v);
       }
       const float4 rv = map4(rinv, gi);
-      const float4 uo = a.init ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(u, gi);
+      const float4 uo = init ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(u, gi);
       const float4 sv = dense_on ? __ldg(reinterpret_cast<const float4*>(ds.field + gi)) : make_float4(0.f, 0.f, 0.f, 0.f);
       const float pmv[4] = {pm.x, pm.y, pm.z, pm.w}, rvv[4] = {rv.x, rv.y, rv.z, rv.w};
       const float uov[4] = {uo.x, uo.y, uo.z, uo.w}, svv[4] = {sv.x, sv.y, sv.z, sv.w};
@@ -700,7 +704,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
       for (int j = 0; j < 4; ++j) {
         const float g = get_comp(G, lay, q, x + j);
         float un;
-        if (a.init)
+        if (init)
           un = a.dt * rvv[j] * g / 2.f;
         else
           un = pmv[j] * (pmv[j] * uov[j] - a.dt * rvv[j] * g);
@@ -725,7 +729,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
       const float pm = __ldg(pml + coord);
       const float rv = rinv.at(gi);
       float un;
-      if (a.init)
+      if (init)
         un = a.dt * rv * g / 2.f;
       else
         un = pm * (pm * u[gi] - a.dt * rv * g);
@@ -737,7 +741,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
   // sparse velocity sources (dirichlet / additive without correction; a
   // transducer is an additive x source with per-point delays and weights)
   const float* ssig = a.src_sig[ax];
-  if (a.src.n > 0 && ssig && t <= a.src_len[ax] && !a.init) {
+  if (!LEAN && a.src.n > 0 && ssig && t <= a.src_len[ax] && !init) {
     const long long rend = min(r0 + 2LL * L, d.row1);
     tile_range(a.src.idx, a.src.n, r0 * nx, rend * nx, sh);
     const int lo = sh[0], hi = sh[1];
@@ -761,7 +765,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
       const float4 v = make_float4(get_comp(G, lay, q, x), get_comp(G, lay, q, x + 1), get_comp(G, lay, q, x + 2),
                                    get_comp(G, lay, q, x + 3));
       st4(u, gi, v);
-      sensor_dense4(s, fi, gi, v);
+      if (!LEAN) sensor_dense4(s, fi, gi, v);
     }
   } else {
 #pragma unroll 4
@@ -775,7 +779,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
       sensor_dense(s, fi, gi, v);
     }
   }
-  sensor_sparse_tile(s, fi, G, lay, d, r0, L, sh);
+  if (!LEAN) sensor_sparse_tile(s, fi, G, lay, d, r0, L, sh);
   if (a.do_r2c) {
     __syncthreads();
     float2* F = tile_fft<NC, false, false>(G, W, tw, plan, L, lay);
@@ -789,7 +793,10 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constan
 // lossless / Stokes EOS (p, sensors, R2C of p) or, for power-law absorption,
 // the local part of p plus the R2C of rho0 * sum(du) and sum(rho).
 // ---------------------------------------------------------------------------
-template <int NC, int DIM>
+// EOSK 1: the variant for power-law absorption without sparse pressure
+// sources (no sensor, Stokes, lossless-EOS or source-pass code: a smaller
+// kernel body); -1: every case, the equation of state read from a.eos.
+template <int NC, int DIM, int EOSK>
 __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x_rho(const __grid_constant__ RhoArgs a, Dims d,
                                                              const __grid_constant__ FFTPlan plan,
                                                              const float2* __restrict__ tw_g, int Lrt) {
@@ -799,6 +806,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
   const int nx = CT ? NC : d.nx;
   const int L = row_lines<NC>(Lrt);
   constexpr int dim = DIM;
+  const int eos = EOSK >= 0 ? EOSK : a.eos;
   const RowLayout lay{row_layout_stride(nx)};
   float2* tw = sm;
   float2* pool[4];
@@ -853,8 +861,8 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
           pf.field(a.rho0.p);
           pf.field(a.c0sq.p);
           if (a.nonlinear) pf.field(a.bona.p);
-          if (a.eos == 2) pf.field(a.tau.p);
-          if (a.eos != 1) pf.sensor(a.sens, fi);
+          if (eos == 2) pf.field(a.tau.p);
+          if (eos != 1) pf.sensor(a.sens, fi);
         }
       }
       if constexpr (RowBulk<NC>::OK) {
@@ -891,11 +899,11 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       if (!used[b]) Wk = pool[b];
   }
 
-  const bool sp = (a.src.n > 0) && (t <= a.src.len);
+  const bool sp = EOSK < 0 && (a.src.n > 0) && (t <= a.src.len);
   const bool dense_on = a.dsrc.field && t <= a.dsrc.len;
   const float damp = dense_on ? (a.dsrc.sig ? __ldg(a.dsrc.sig + t - 1) : 1.f) : 0.f;
   const int total = 2 * L * nx;
-  const bool absorbing = (a.eos == 1);
+  const bool absorbing = (eos == 1);
 
   constexpr bool VEC = NC > 0 && NC % 4 == 0;
   if (VEC && !sp) {
@@ -931,7 +939,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       const float4 r0v4 = map4(a.rho0, gi);
       const float4 c24 = map4(a.c0sq, gi);
       const float4 bn4 = a.nonlinear ? map4(a.bona, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 ta4 = (a.eos == 2) ? map4(a.tau, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 ta4 = (eos == 2) ? map4(a.tau, gi) : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 ds4 = dense_on ? __ldg(reinterpret_cast<const float4*>(a.dsrc.field + gi))
                                   : make_float4(0.f, 0.f, 0.f, 0.f);
       Acc4 acc;  // the sensor accumulators (lossless / Stokes), loaded before any store
@@ -971,7 +979,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
           if (dim == 3) rsum += rn[2][j];
         }
         float term = rsum;
-        if (a.eos == 2) term = term + c(ta4) * r0v * dsum;
+        if (eos == 2) term = term + c(ta4) * r0v * dsum;
         if (a.nonlinear) term = term + c(bn4) * rsum * rsum / (2.f * r0v);
         outp[j] = c(c24) * term;
         outq[j] = r0v * dsum;
@@ -1078,7 +1086,7 @@ __global__ void __launch_bounds__(RTile<NC>::THREADS, RTile<NC>::MIN_BLOCKS) k_x
       // equation of state (kspaceFirstOrder3D.m:963-1017)
       const float c2 = a.c0sq.at(gi);
       float term = rsum;
-      if (a.eos == 2) term = term + a.tau.at(gi) * r0v * dsum;
+      if (eos == 2) term = term + a.tau.at(gi) * r0v * dsum;
       if (a.nonlinear) term = term + a.bona.at(gi) * rsum * rsum / (2.f * r0v);
       const float pv = c2 * term;
       if (absorbing) {
@@ -1382,8 +1390,13 @@ template <int NC>
 static void x_u_t(const UArgs& a, const Dims& d, const FFTPlan& plan, const float2* tw, int Lrt, cudaStream_t st) {
   const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? 1 : 2);
-  set_smem(k_x_u<NC>, sm);
-  launch_pdl(k_x_u<NC>, dim3(row_tiles(d, L), d.dim), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
+  bool lean = !a.init && a.src.n == 0;
+  for (int ax = 0; ax < d.dim; ++ax) lean = lean && !a.dsrc[ax].field && a.sens[ax].mode == 0;
+  auto go = [&](auto k) {
+    set_smem(k, sm);
+    launch_pdl(k, dim3(row_tiles(d, L), d.dim), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
+  };
+  lean ? go(k_x_u<NC, true>) : go(k_x_u<NC, false>);
 }
 
 template <int NC>
@@ -1391,13 +1404,15 @@ static void x_rho_t(const RhoArgs& a, const Dims& d, const FFTPlan& plan, const 
                     cudaStream_t st) {
   const int L = NC > 0 ? RTile<NC>::LINES : Lrt;
   const size_t sm = smem_row(d.nx, L, NC > 0 ? d.dim : d.dim + 1);
-  if (d.dim == 3) {
-    set_smem(k_x_rho<NC, 3>, sm);
-    launch_pdl(k_x_rho<NC, 3>, dim3(row_tiles(d, L)), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
-  } else {
-    set_smem(k_x_rho<NC, 2>, sm);
-    launch_pdl(k_x_rho<NC, 2>, dim3(row_tiles(d, L)), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
-  }
+  auto go = [&](auto k) {
+    set_smem(k, sm);
+    launch_pdl(k, dim3(row_tiles(d, L)), dim3(RTile<NC>::THREADS), sm, st, a, d, plan, tw, L);
+  };
+  const bool lean = a.eos == 1 && a.src.n == 0;
+  if (d.dim == 3)
+    lean ? go(k_x_rho<NC, 3, 1>) : go(k_x_rho<NC, 3, -1>);
+  else
+    lean ? go(k_x_rho<NC, 2, 1>) : go(k_x_rho<NC, 2, -1>);
 }
 
 template <int NC>
