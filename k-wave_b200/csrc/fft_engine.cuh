@@ -29,12 +29,37 @@ struct FFTPlan {
   int rad[KWB_MAX_STAGES];    // radix of each stage
 };
 
-__host__ __device__ inline float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__host__ __device__ inline float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// On sm_100 the complex additions and scalings issue as packed FP32x2
+// instructions (one instruction for both components; per component the
+// same IEEE rounding as the scalar form: a - b as fma(b, -1, a) is exact
+// before its one rounding).
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && !defined(KWB_NO_F32X2)
+#define KWB_F32X2 1
+#endif
+__host__ __device__ inline float2 c_add(float2 a, float2 b) {
+#ifdef KWB_F32X2
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__host__ __device__ inline float2 c_sub(float2 a, float2 b) {
+#ifdef KWB_F32X2
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
 __host__ __device__ inline float2 c_mul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__host__ __device__ inline float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ inline float2 c_scale(float2 a, float s) {
+#ifdef KWB_F32X2
+  return __fmul2_rn(a, make_float2(s, s));
+#else
+  return make_float2(a.x * s, a.y * s);
+#endif
+}
 __host__ __device__ inline float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>

@@ -609,9 +609,11 @@ struct RawRows {
 // ---------------------------------------------------------------------------
 // LEAN: the variant for steps with no velocity source and no velocity sensor
 // after the first (no source, sensor or initial-pressure code: a smaller
-// kernel body); otherwise every case.
+// kernel body), held to 64 registers a thread (8 blocks of 128 threads per
+// SM at 256 points); otherwise every case, held to 72 (7 blocks).
 template <int NC, bool LEAN>
-__global__ void __launch_bounds__(RTile<NC>::THREADS) k_x_u(const __grid_constant__ UArgs a, Dims d,
+__global__ void __launch_bounds__(RTile<NC>::THREADS, NC > 0 ? 65536 / (RTile<NC>::THREADS * (LEAN ? 64 : 72)) : 1)
+    k_x_u(const __grid_constant__ UArgs a, Dims d,
                                                            const __grid_constant__ FFTPlan plan,
                                                            const float2* __restrict__ tw_g, int Lrt) {
   extern __shared__ __align__(16) float2 sm[];
