@@ -609,10 +609,13 @@ struct RawRows {
 // ---------------------------------------------------------------------------
 // LEAN: the variant for steps with no velocity source and no velocity sensor
 // after the first (no source, sensor or initial-pressure code: a smaller
-// kernel body), held to 64 registers a thread (8 blocks of 128 threads per
-// SM at 256 points); otherwise every case, held to 72 (7 blocks).
+// kernel body); otherwise every case.  At 256 points the lean variant is
+// held to 64 registers a thread (8 blocks of 128 threads per SM) and the
+// general one to 72 (7 blocks); other lengths keep the compiler's own
+// choice (a minimum block count of 0 sets no bound), which caps would push
+// into spills (96, 128, 160, 192 points).
 template <int NC, bool LEAN>
-__global__ void __launch_bounds__(RTile<NC>::THREADS, NC > 0 ? 65536 / (RTile<NC>::THREADS * (LEAN ? 64 : 72)) : 1)
+__global__ void __launch_bounds__(RTile<NC>::THREADS, NC == 256 ? (LEAN ? 8 : 7) : 0)
     k_x_u(const __grid_constant__ UArgs a, Dims d,
                                                            const __grid_constant__ FFTPlan plan,
                                                            const float2* __restrict__ tw_g, int Lrt) {
