@@ -148,6 +148,9 @@ def test_session_bytes_counts_recorded_outputs():
     assert serving.session_bytes(inp, ("p",), Sz) - serving.session_bytes(inp, (), Sz) == 4 * 10 * 100
     assert serving.session_bytes(inp, ("u",), Sz) - serving.session_bytes(inp, (), Sz) == 2 * 4 * 10 * 100
     assert serving.session_bytes(inp, ("p_final",), Sz) - serving.session_bytes(inp, (), Sz) == 4 * 1000
+    # rms: a Kahan pair of the completed blocks and the open block's partial sum per sensor point
+    assert serving.session_bytes(inp, ("p_rms",), Sz) - serving.session_bytes(inp, (), Sz) == 12 * 10
+    assert serving.session_bytes(inp, ("u_rms",), Sz) - serving.session_bytes(inp, (), Sz) == 2 * 12 * 10
     assert base >= 5000
 
 
